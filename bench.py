@@ -1,0 +1,471 @@
+#!/usr/bin/env python3
+"""Benchmark of the plain FFMA SGEMM path (and the split-precision paths beside it).
+
+Workload (one step = one GEMM):  C := 1.5 * A @ B + 0.5 * C, FP32 row-major,
+M = N = K = 8192, A, B, C uniform[-1, 1) from the seeded generator (seed 0) --
+the 8192^3 point of the plain FFMA square sweep with alpha=1.5, beta=0.5.
+Inputs are 768 MB, larger than the 126 MB L2, and each timed step is bracketed
+by its own CUDA events with an L2-sized flush write in between steps.
+
+  value        device-timed GFLOP/s, operands resident in HBM (max over ranks)
+  e2e          the same GEMM through the C ABI from pinned HOST buffers: H2D of
+               A, B, C, the GEMM, D2H of C -- all inside the timed region
+  roofline     FP32 SIMT peak = SMs x 128 FMA lanes x 2 x SM clock
+  cpu_baseline the oracle (C restatement of the reference's kernel_basic,
+               OpenMP on the host cores) on a bounded sample of rows of the same
+               workload; the same leg checks the GPU rows bit for bit
+  split        BF16x6 / TF32x3 tensor-core paths on the same 8192^3 problem,
+               GFLOP/s and error against FP64 on sampled rows
+
+`--impl reference` runs the reference's own sgemm() (its 128x256x8 kernel at
+this size) built from its sources for sm_100a, same workload and metric.
+
+Multi-GPU: replicas (the GEMM has no exchange step in this scope); each rank
+runs the same workload on its GPU, timing is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "sgemm.cu_b200"))
+
+SIZE = 8192
+ALPHA, BETA = 1.5, 0.5
+SEED = 0
+
+
+# ------------------------------------------------------------------ helpers --
+
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = os.path.join("/tmp", f"sgemm_b200_clocks_{os.getpid()}.csv")
+
+    def start(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.f,
+                stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        sm, smax, reasons, power = [], None, set(), []
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sm.append(float(parts[1]))
+                    smax = float(parts[2])
+                    power.append(float(parts[3]))
+                except ValueError:
+                    continue
+                for nm, v in zip(names, parts[5:9]):
+                    if v.lower().startswith("active"):
+                        reasons.add(nm)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "samples": len(sm), "power_w_max": max(power) if power else None,
+                "reasons": sorted(reasons)}
+
+
+def _dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def _init_dist(world: int, local: int):
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+    if world > 1:
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    return dist if world > 1 else None
+
+
+def _max_over_ranks(dist, value: float) -> float:
+    if dist is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def _barrier(dist):
+    import torch
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f), "measured"
+    except Exception:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0,
+                "sm_max_mhz": 1965.0}, "fallback"
+
+
+def _traffic(kernel_key: str):
+    """DRAM bytes per launch of the dominant kernel from the committed ncu summary."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            return json.load(f).get(kernel_key)
+    except Exception:
+        return None
+
+
+# -------------------------------------------------------------- device legs --
+
+def _alloc_inputs(torch, sg, size):
+    A = torch.empty((size, size), device="cuda")
+    B = torch.empty((size, size), device="cuda")
+    C = torch.empty((size, size), device="cuda")
+    sg.fill_random(A, SEED, 1, sg.DIST_UNIFORM_PM1)
+    sg.fill_random(B, SEED, 2, sg.DIST_UNIFORM_PM1)
+    sg.fill_random(C, SEED, 3, sg.DIST_UNIFORM_PM1)
+    return A, B, C
+
+
+def _time_steps(torch, fn, steps, warmup, flush):
+    """Per-step CUDA-event times (ms) on the current stream; flush L2 between steps."""
+    stream = torch.cuda.current_stream()
+    for _ in range(warmup):
+        fn()
+        flush.add_(1)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(steps)]
+    torch.cuda.synchronize()
+    for s, e in ev:
+        s.record(stream)
+        fn()
+        e.record(stream)
+        flush.add_(1)
+    torch.cuda.synchronize()
+    return [s.elapsed_time(e) for s, e in ev]
+
+
+def _e2e(torch, gemm_host, steps, warmup, size):
+    """GEMM from pinned host buffers: H2D(A,B,C) + GEMM + D2H(C), per step."""
+    hA = torch.empty((size, size), dtype=torch.float32, pin_memory=True)
+    hB = torch.empty((size, size), dtype=torch.float32, pin_memory=True)
+    hC = torch.empty((size, size), dtype=torch.float32, pin_memory=True)
+    hA.uniform_(-1, 1)
+    hB.uniform_(-1, 1)
+    hC.uniform_(-1, 1)
+    hOut = torch.empty((size, size), dtype=torch.float32, pin_memory=True)
+    dA = torch.empty((size, size), device="cuda")
+    dB = torch.empty_like(dA)
+    dC = torch.empty_like(dA)
+
+    def step():
+        dA.copy_(hA, non_blocking=True)
+        dB.copy_(hB, non_blocking=True)
+        dC.copy_(hC, non_blocking=True)
+        gemm_host(dA, dB, dC)
+        hOut.copy_(dC, non_blocking=True)
+
+    for _ in range(warmup):
+        step()
+    torch.cuda.synchronize()
+    s = torch.cuda.Event(enable_timing=True)
+    e = torch.cuda.Event(enable_timing=True)
+    s.record()
+    for _ in range(steps):
+        step()
+    e.record()
+    torch.cuda.synchronize()
+    ms = s.elapsed_time(e) / steps
+    return ms, 3 * size * size * 4, size * size * 4
+
+
+def _cpu_baseline_and_parity(torch, sg, C_after, C0_rows, rows, size, target_s=10.0):
+    """Oracle (kernel_basic restatement) on sampled rows: timing + exact check."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    hA = oracle.fill(size, size, SEED, 1, 0)
+    hB = oracle.fill(size, size, SEED, 2, 0)
+    threads = oracle.max_threads()
+    # calibrate on 8 rows, then run about target_s seconds of rows
+    t0 = time.perf_counter()
+    oracle.sgemm_basic_rows(rows[:8], hA, hB, C0_rows[:8], ALPHA, BETA,
+                            read_c_if_beta_zero=False)
+    per_row = (time.perf_counter() - t0) / 8
+    nrows = int(max(8, min(len(rows), target_s / max(per_row, 1e-6))))
+    t0 = time.perf_counter()
+    out = oracle.sgemm_basic_rows(rows[:nrows], hA, hB, C0_rows[:nrows], ALPHA, BETA,
+                                  read_c_if_beta_zero=False)
+    dt = time.perf_counter() - t0
+    gflops = 2.0 * nrows * size * size / dt * 1e-9
+    got = C_after[:nrows]
+    exact = int(np.sum(got == out))
+    # FP64 error of the plain path on the same rows
+    ref, mag = oracle.dgemm(hA, hB, C0_rows[:nrows], ALPHA, BETA,
+                            row_ids=rows[:nrows])
+    err = oracle.error_stats(got, ref, mag)
+    return {
+        "value": round(gflops, 2), "unit": "GFLOP/s", "cores": threads, "kind": "port",
+        "sample": f"{nrows} of {size} rows of the {size}^3 GEMM (kernel_basic restatement, "
+                  f"fmaf chain, OpenMP over rows)",
+        "seconds": round(dt, 2),
+        "parity": {"rows_checked": nrows, "elements": int(got.size), "bit_exact": exact},
+        "plain_error_vs_fp64": {k: float(v) for k, v in err.items()},
+    }, (hA, hB)
+
+
+def _split_leg(torch, sg, A, B, C0, flush, steps, warmup, rows, host_ab, peaks):
+    """BF16x6 / TF32x3 on the same problem: GFLOP/s and sampled-row FP64 error."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    out = {}
+    hA, hB = host_ab
+    idx = torch.from_numpy(rows).long().cuda()
+    C0_rows = C0[idx].cpu().numpy()
+    ref, mag = oracle.dgemm(hA, hB, C0_rows, ALPHA, BETA, row_ids=rows)
+    for name in ("bf16x6", "tf32x3"):
+        path = sg.PATHS[name]
+        try:
+            ws = torch.empty(sg.split_workspace_size(path, SIZE, SIZE, SIZE), dtype=torch.uint8,
+                             device="cuda")
+            C = C0.clone()
+            sg.sgemm_split(path, A, B, C, ALPHA, BETA, workspace=ws)
+            torch.cuda.synchronize()
+            err = oracle.error_stats(C[idx].cpu().numpy(), ref, mag)
+
+            def run():
+                sg.sgemm_split(path, A, B, C, ALPHA, BETA, workspace=ws)
+
+            ms = _time_steps(torch, run, steps, warmup, flush)
+            t = statistics.mean(ms)
+            gf = 2.0 * SIZE ** 3 / (t * 1e-3) * 1e-9
+            prods = 6 if name == "bf16x6" else 3
+            tc_peak = peaks["bf16_tflops"] * (1.0 if name == "bf16x6" else 0.5)
+            out[name] = {"gflops": round(gf, 1), "ms_per_step": round(t, 4),
+                         "useful_roofline_tflops": round(tc_peak / prods, 1),
+                         "frac_of_useful_roofline": round(gf * 1e-3 / (tc_peak / prods), 4),
+                         "error_vs_fp64_sampled_rows": {k: float(v) for k, v in err.items()}}
+            del ws
+        except Exception as e:  # report, never hide
+            out[name] = {"error": str(e)}
+    return out
+
+
+# --------------------------------------------------------------------- main --
+
+def run(args):
+    import torch
+    rank, world, local = _dist_env()
+    torch.cuda.set_device(local)
+    dist = _init_dist(world, local)
+    peaks, peak_src = _peaks()
+    props = torch.cuda.get_device_properties(local)
+    sms = props.multi_processor_count
+
+    if args.impl == "reference":
+        if rank != 0:
+            if dist is not None:
+                dist.destroy_process_group()
+            return
+        return run_reference(args, torch, peaks, sms, local)
+
+    import sgemm_b200 as sg
+    A, B, C = _alloc_inputs(torch, sg, SIZE)
+    C0 = C.clone()
+    flush = torch.empty(int(peaks.get("l2_bytes", 256 << 20)) // 4, device="cuda")
+    cfg = sg.select_config(SIZE, SIZE, SIZE, A, SIZE, B, SIZE)
+    cfg_name = sg.config_names()[cfg]
+
+    # parity sample: rows of C after one GEMM from C0
+    rows = np.linspace(0, SIZE - 1, 512).astype(np.int32)
+    idx = torch.from_numpy(rows).long().cuda()
+    C0_rows = C0[idx].cpu().numpy()
+    sg.sgemm(A, B, C, ALPHA, BETA)
+    torch.cuda.synchronize()
+    C_after = C[idx].cpu().numpy()
+    C.copy_(C0)
+
+    def step():
+        sg.sgemm(A, B, C, ALPHA, BETA)
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    for _ in range(args.warmup):
+        step()
+        flush.add_(1)
+    _barrier(dist)
+    ms = _time_steps(torch, step, args.steps, 0, flush)
+    _barrier(dist)
+    clk = clocks.stop()
+    total_ms = _max_over_ranks(dist, sum(ms))
+    ms_step = total_ms / args.steps
+    flops = 2.0 * SIZE ** 3
+    value = flops * world * args.steps / (total_ms * 1e-3) * 1e-9  # GFLOP/s, whole job
+
+    # roofline: FP32 SIMT peak (SMs x 128 FMA/clk x 2) at max and observed clock
+    sm_max = clk.get("sm_max_mhz") or peaks.get("sm_max_mhz", 1965.0)
+    sm_obs = clk.get("sm_mhz") or sm_max
+    per_launch_gflops = flops / (statistics.mean(ms) * 1e-3) * 1e-9
+    peak_max = sms * 256 * sm_max * 1e-3  # GFLOP/s
+    peak_obs = sms * 256 * sm_obs * 1e-3
+    roofline = {
+        "bound": "fp32_simt", "unit": "TFLOP/s",
+        "achieved": round(per_launch_gflops * 1e-3, 2),
+        "peak": round(peak_max * 1e-3, 2),
+        "frac": round(per_launch_gflops / peak_max, 4),
+        "peak_at_observed_clock": round(peak_obs * 1e-3, 2),
+        "frac_at_observed_clock": round(per_launch_gflops / peak_obs, 4),
+        "peak_source": f"computed: {sms} SMs x 128 FP32 lanes x 2 FLOP x SM clock "
+                       f"(max {sm_max:.0f} MHz, observed median {sm_obs:.0f} MHz)",
+        "kernel": cfg_name,
+        "traffic": _traffic(cfg_name),
+        "algorithmic_bytes": 4 * 4 * SIZE * SIZE,
+    }
+
+    result = {
+        "metric": f"plain FFMA SGEMM GFLOP/s at M=N=K={SIZE} (alpha=1.5, beta=0.5)",
+        "value": round(value, 1), "unit": "GFLOP/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms_step, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"sgemm_plain_{SIZE}", "m": SIZE, "n": SIZE, "k": SIZE,
+                   "alpha": ALPHA, "beta": BETA, "dist": "uniform[-1,1) seed 0",
+                   "layout": "row-major NN", "kernel_config": cfg_name,
+                   "l2": "inputs 768 MB > 126 MB L2, plus an L2-sized flush between steps",
+                   "parallelism": f"replicas x{world}"},
+        "p50_ms": round(statistics.median(ms), 4),
+        "p99_ms": round(sorted(ms)[min(len(ms) - 1, int(0.99 * len(ms)))], 4),
+        "roofline": roofline,
+        "clocks": clk,
+        "gpu_launches": args.steps,
+        "peaks_source": peak_src,
+    }
+
+    # e2e through the C ABI from pinned host buffers
+    if not args.skip_e2e:
+        ms_e2e, h2d, d2h = _e2e(torch, lambda a, b, c: sg.sgemm(a, b, c, ALPHA, BETA),
+                                max(3, args.steps // 5), 2, SIZE)
+        e2e_ms = _max_over_ranks(dist, ms_e2e)
+        result["e2e"] = {"value": round(flops * world / (e2e_ms * 1e-3) * 1e-9, 1),
+                         "unit": "GFLOP/s", "ms_per_step": round(e2e_ms, 3),
+                         "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h}
+
+    if rank == 0 and world == 1 and not args.skip_cpu:
+        cpu, host_ab = _cpu_baseline_and_parity(torch, sg, C_after, C0_rows, rows, SIZE,
+                                                target_s=args.cpu_seconds)
+        result["cpu_baseline"] = cpu
+        if not args.skip_split:
+            result["split"] = _split_leg(torch, sg, A, B, C0, flush, max(3, args.steps // 2),
+                                         args.warmup, rows[:64], host_ab, peaks)
+    if rank == 0:
+        print(json.dumps(result))
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def run_reference(args, torch, peaks, sms, local):
+    """The reference's own sgemm() built from its sources, same workload."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    try:
+        oracle.ref()
+    except Exception as e:
+        print(json.dumps({"impl": "reference", "unavailable": f"reference build missing: {e}"}))
+        return
+    import sgemm_b200 as sg  # only for the seeded fill of the inputs
+    A, B, C = _alloc_inputs(torch, sg, SIZE)
+    flush = torch.empty((256 << 20) // 4, device="cuda")
+
+    def step():
+        oracle.ref_sgemm(A, B, C, ALPHA, BETA)
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    ms = _time_steps(torch, step, args.steps, args.warmup, flush)
+    clk = clocks.stop()
+    flops = 2.0 * SIZE ** 3
+    t = statistics.mean(ms)
+    value = flops / (t * 1e-3) * 1e-9
+    ms_e2e, h2d, d2h = _e2e(torch, lambda a, b, c: oracle.ref_sgemm(a, b, c, ALPHA, BETA),
+                            max(3, args.steps // 5), 2, SIZE)
+    sm_max = clk.get("sm_max_mhz") or peaks.get("sm_max_mhz", 1965.0)
+    peak = sms * 256 * sm_max * 1e-3
+    result = {
+        "impl": "reference",
+        "metric": "plain FFMA SGEMM GFLOP/s at M=N=K=8192 (alpha=1.5, beta=0.5)",
+        "value": round(value, 1), "unit": "GFLOP/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(t, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "sgemm_plain_8192", "m": SIZE, "n": SIZE, "k": SIZE,
+                   "alpha": ALPHA, "beta": BETA, "dist": "uniform[-1,1) seed 0",
+                   "kernel_config": "reference sgemm_128x256x8 (src/sgemm.cuh:41-44)",
+                   "l2": "inputs 768 MB > 126 MB L2, plus an L2-sized flush between steps"},
+        "roofline": {"bound": "fp32_simt", "unit": "TFLOP/s", "achieved": round(value * 1e-3, 2),
+                     "peak": round(peak * 1e-3, 2), "frac": round(value / peak, 4),
+                     "traffic": None},
+        "clocks": clk,
+        "e2e": {"value": round(flops / (ms_e2e * 1e-3) * 1e-9, 1), "unit": "GFLOP/s",
+                "ms_per_step": round(ms_e2e, 3), "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h},
+        "cpu_baseline": {"value": round(value, 1), "unit": "GFLOP/s", "cores": None,
+                         "kind": "reference",
+                         "sample": "the reference has no CPU GEMM (its test oracle is the GPU "
+                                   "kernel_basic); this arm runs its own sgemm() kernels, built "
+                                   "from its sources for sm_100a, on the B200"},
+    }
+    print(json.dumps(result))
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=40)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--skip-split", action="store_true")
+    ap.add_argument("--skip-e2e", action="store_true")
+    ap.add_argument("--size", type=int, default=SIZE,
+                    help="M=N=K (default 8192; smaller sizes only for profiler captures)")
+    args = ap.parse_args()
+    globals()["SIZE"] = args.size
+    if args.warmup < 3:
+        args.warmup = 3
+    run(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,208 @@
+/*
+ * sgemm_b200.h — C ABI of the B200-native (sm_100a) FP32 GEMM library.
+ *
+ *   C := alpha * A * B + beta * C        (FP32, row-major, "NN")
+ *
+ * A is m x k with row stride lda, B is k x n with row stride ldb, C is m x n
+ * with row stride ldc, all in elements.  Matrices are caller-owned DEVICE
+ * pointers; alpha and beta are caller-owned HOST pointers read by value when
+ * the call is made (the reference's convention, src/sgemm.cuh:19-30,44,47).
+ * Column-major callers swap (A, lda) and (B, ldb) and exchange m and n,
+ * because C^T = B^T * A^T (src/sgemm.cuh:31-33).
+ *
+ * Every entry point returns an sgemm_b200_status.  Work is enqueued on the
+ * given stream and the call returns without synchronising, like the
+ * reference's sgemm() (src/sgemm.cuh:35-48), which also never synchronises.
+ *
+ * Unlike the reference kernels (128x128x8.cuh:263,368 and 128x256x8.cuh:273,
+ * 372-380 use n for the B and C row strides), every path here honours general
+ * lda >= k, ldb >= n and ldc >= n.  With beta == 0, C is never read, matching
+ * the reference's tiled kernels (128x256x8.cuh:365-380).
+ */
+#ifndef SGEMM_B200_H
+#define SGEMM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* cudaStream_t without pulling in the CUDA headers: the ABI takes it as an
+ * opaque pointer (NULL = the legacy default stream). */
+typedef void* sgemm_b200_stream_t;
+
+typedef enum {
+    SGEMM_B200_OK = 0,
+    SGEMM_B200_ERR_INVALID_ARG = 1,   /* negative size, ld too small, NULL pointer */
+    SGEMM_B200_ERR_UNSUPPORTED = 2,   /* no sm_100 device, or mode not built */
+    SGEMM_B200_ERR_CUDA = 3,          /* a CUDA runtime/driver call failed */
+    SGEMM_B200_ERR_TIMEOUT = 4,       /* a bounded device-side wait expired */
+    SGEMM_B200_ERR_NO_MEMORY = 5,     /* allocation or workspace too small */
+    SGEMM_B200_ERR_REJECTED = 6       /* serving: request refused by admission */
+} sgemm_b200_status;
+
+/* Compute paths. */
+typedef enum {
+    SGEMM_B200_PATH_PLAIN = 0,    /* FFMA on the SIMT pipes, bit-exact with the reference */
+    SGEMM_B200_PATH_BF16X6 = 1,   /* 3-way BF16 split, 6 cross products on tcgen05 */
+    SGEMM_B200_PATH_TF32X3 = 2    /* 2-way TF32 split, 3 cross products on tcgen05 */
+} sgemm_b200_path;
+
+/* ------------------------------------------------------------------------ */
+/* Plain FFMA path                                                           */
+/* ------------------------------------------------------------------------ */
+
+/* Replaces sgemm() at src/sgemm.cuh:19-48 (the GPUCC >= 80 branch that
+ * launches sgemm_128x128x8 / sgemm_128x256x8), adding a stream argument and a
+ * status return.  Each C element is accumulated over k in increasing order
+ * with one fused multiply-add per term, then acc *= alpha and
+ * C = fmaf(C_old, beta, acc), so results equal the reference kernels' bit for
+ * bit on the same inputs. */
+int sgemm_b200(int m, int n, int k,
+               const float* alpha,
+               const float* A, int lda,
+               const float* B, int ldb,
+               const float* beta,
+               float* C, int ldc,
+               sgemm_b200_stream_t stream);
+
+/* Same computation with an explicit kernel configuration (see
+ * sgemm_b200_config_count / sgemm_b200_config_name); cfg < 0 means the
+ * dispatcher's choice.  Used by the autotuner and the tests. */
+int sgemm_b200_with_config(int cfg, int m, int n, int k,
+                           const float* alpha,
+                           const float* A, int lda,
+                           const float* B, int ldb,
+                           const float* beta,
+                           float* C, int ldc,
+                           sgemm_b200_stream_t stream);
+
+/* Number of compiled plain-path kernel configurations and their names
+ * (e.g. "tma_128x256_s4"). */
+int sgemm_b200_config_count(void);
+const char* sgemm_b200_config_name(int cfg);
+/* Configuration the dispatcher picks for this shape and these pointers. */
+int sgemm_b200_select_config(int m, int n, int k,
+                             const float* A, int lda,
+                             const float* B, int ldb,
+                             const float* C, int ldc);
+
+/* Replaces sgemm_basic() at src/sgemm.cuh:92-113 (kernel_basic,
+ * src/kernels/basic.cuh:1-26): one thread per C element, sequential
+ * accumulation, C always read.  Kept for the reference's test semantics. */
+int sgemm_b200_basic(int m, int n, int k,
+                     const float* alpha,
+                     const float* A, int lda,
+                     const float* B, int ldb,
+                     const float* beta,
+                     float* C, int ldc,
+                     sgemm_b200_stream_t stream);
+
+/* ------------------------------------------------------------------------ */
+/* Split-precision tensor-core path (no reference counterpart)               */
+/* ------------------------------------------------------------------------ */
+
+/* Bytes of device workspace sgemm_b200_split needs for this shape/path. */
+size_t sgemm_b200_split_workspace_size(int path, int m, int n, int k);
+
+/* C := alpha*A*B + beta*C with A and B split into BF16 (path BF16X6) or TF32
+ * (path TF32X3) terms whose cross products run on tcgen05 with FP32
+ * accumulation in tensor memory.  Same argument meaning as sgemm_b200.
+ * workspace may be NULL, in which case the call allocates it stream-ordered
+ * (cudaMallocAsync/cudaFreeAsync on `stream`). */
+int sgemm_b200_split(int path, int m, int n, int k,
+                     const float* alpha,
+                     const float* A, int lda,
+                     const float* B, int ldb,
+                     const float* beta,
+                     float* C, int ldc,
+                     void* workspace, size_t workspace_bytes,
+                     sgemm_b200_stream_t stream);
+
+/* Dispatch by path: PLAIN goes to sgemm_b200, the others to sgemm_b200_split
+ * with a stream-ordered workspace. */
+int sgemm_b200_gemm(int path, int m, int n, int k,
+                    const float* alpha,
+                    const float* A, int lda,
+                    const float* B, int ldb,
+                    const float* beta,
+                    float* C, int ldc,
+                    sgemm_b200_stream_t stream);
+
+/* ------------------------------------------------------------------------ */
+/* Grouped persistent GEMM (no reference counterpart)                        */
+/* ------------------------------------------------------------------------ */
+
+typedef struct {
+    int m, n, k;
+    int lda, ldb, ldc;
+    float alpha, beta;
+    const float* A;
+    const float* B;
+    float* C;
+} sgemm_b200_problem;
+
+/* Opaque plan: problem table on the device, tile schedule, split-K choice per
+ * problem, and (after the first launch) a captured CUDA graph. */
+typedef struct sgemm_b200_grouped_plan sgemm_b200_grouped_plan;
+
+/* Build a plan for `count` problems (host array, copied).  tuning_json may be
+ * NULL (built-in choices) or a path written by sgemm_b200_autotune_grouped. */
+int sgemm_b200_grouped_plan_create(sgemm_b200_grouped_plan** plan,
+                                   const sgemm_b200_problem* problems, int count,
+                                   const char* tuning_json);
+/* One persistent launch over every problem of the plan on `stream`.
+ * use_graph != 0 replays a CUDA graph captured on the first call. */
+int sgemm_b200_grouped_plan_launch(sgemm_b200_grouped_plan* plan,
+                                   sgemm_b200_stream_t stream, int use_graph);
+/* Tiles and work items in the plan's schedule (for tests and reports). */
+int sgemm_b200_grouped_plan_info(const sgemm_b200_grouped_plan* plan,
+                                 int* tiles, int* work_items, int* grid_ctas);
+void sgemm_b200_grouped_plan_destroy(sgemm_b200_grouped_plan* plan);
+
+/* One-shot convenience: plan, launch once, destroy. */
+int sgemm_b200_grouped(const sgemm_b200_problem* problems, int count,
+                       sgemm_b200_stream_t stream);
+
+/* Time the candidate tile/stage/split-K choices per size bucket on the current
+ * device with the given problems and write the winners to json_path. */
+int sgemm_b200_autotune_grouped(const sgemm_b200_problem* problems, int count,
+                                const char* json_path);
+
+/* ------------------------------------------------------------------------ */
+/* Utilities                                                                 */
+/* ------------------------------------------------------------------------ */
+
+/* Distributions of the seeded counter-based generator. */
+typedef enum {
+    SGEMM_B200_DIST_UNIFORM_PM1 = 0,  /* uniform[-1, 1) */
+    SGEMM_B200_DIST_UNIFORM_01 = 1,   /* uniform[0, 1)  (the reference's init_random) */
+    SGEMM_B200_DIST_SIGNED_POW2 = 2   /* random sign * 2^e * uniform[1,2), e in [-10, 10] */
+} sgemm_b200_dist;
+
+/* Fill rows x cols (row stride ld) of a device matrix with value
+ * f(seed, tag, row*cols + col) of the chosen distribution.  The same values
+ * come out of the host generator in the oracle, bit for bit. */
+int sgemm_b200_fill_random(float* X, int rows, int cols, int ld,
+                           uint64_t seed, uint32_t tag, int dist,
+                           sgemm_b200_stream_t stream);
+
+/* Reads and clears the device-side status word that bounded waits set on
+ * expiry (SGEMM_B200_OK or SGEMM_B200_ERR_TIMEOUT).  Synchronises the device. */
+int sgemm_b200_device_status(void);
+
+/* Status of the most recent call on this thread (used by sgemm(), which
+ * returns void like the reference). */
+int sgemm_b200_last_status(void);
+const char* sgemm_b200_status_string(int status);
+
+/* Library version string. */
+const char* sgemm_b200_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SGEMM_B200_H */

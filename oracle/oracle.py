@@ -1,0 +1,196 @@
+"""TEST INFRASTRUCTURE ONLY: ctypes binding of the oracle libraries.
+
+  liboracle.so       CPU restatement of kernel_basic (reference
+                     src/kernels/basic.cuh:14-25), FP64 GEMM, error stats, and
+                     the seeded generator (oracle.c)
+  liboracle_gpu.so   FP64 GEMM on the GPU for 8192^3 / 16384^3 accuracy checks
+  _ref/libref_sgemm.so
+                     the reference's own sgemm()/sgemm_basic() compiled for
+                     sm_100a from its sources (ref_sgemm.cu)
+
+Only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline leg (and its
+reference arm, which times the reference itself) may use this module, and only
+as the checker or as the thing being compared against.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Optional
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CPU_LIB = os.path.join(HERE, "liboracle.so")
+GPU_LIB = os.path.join(HERE, "liboracle_gpu.so")
+REF_LIB = os.path.join(HERE, "_ref", "libref_sgemm.so")
+
+_cpu = None
+_gpu = None
+_ref = None
+
+_F32P = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
+_F64P = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+_I32P = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+_I = ctypes.c_int
+
+
+def cpu() -> ctypes.CDLL:
+    global _cpu
+    if _cpu is None:
+        l = ctypes.CDLL(CPU_LIB)
+        l.oracle_fill.argtypes = [_F32P, _I, _I, _I, ctypes.c_uint64, ctypes.c_uint32, _I]
+        l.oracle_fill_rows.argtypes = [_F32P, _I32P, _I, _I, ctypes.c_uint64, ctypes.c_uint32, _I]
+        l.oracle_sgemm_basic.argtypes = [_I, _I, _I, ctypes.c_float, _F32P, _I, _F32P, _I,
+                                         ctypes.c_float, _F32P, _I, _I, _I]
+        l.oracle_sgemm_basic_rows.argtypes = [_I, _I32P, _I, _I, ctypes.c_float, _F32P, _I, _F32P,
+                                              _I, ctypes.c_float, _F32P, _I, _I, _I]
+        l.oracle_dgemm_rows.argtypes = [_I, ctypes.c_void_p, _I, _I, ctypes.c_double, _F32P, _I,
+                                        _F32P, _I, ctypes.c_double, ctypes.c_void_p, _I, _F64P,
+                                        ctypes.c_void_p, _I]
+        l.oracle_error_stats.argtypes = [ctypes.c_int64, _F32P, _F64P, ctypes.c_void_p, _F64P]
+        l.oracle_max_threads.restype = _I
+        _cpu = l
+    return _cpu
+
+
+def max_threads() -> int:
+    return cpu().oracle_max_threads()
+
+
+def fill(rows: int, cols: int, seed: int, tag: int, dist: int) -> np.ndarray:
+    X = np.empty((rows, cols), dtype=np.float32)
+    if rows and cols:
+        assert cpu().oracle_fill(X, rows, cols, cols, seed, tag, dist) == 0
+    return X
+
+
+def fill_rows(row_ids, cols: int, seed: int, tag: int, dist: int) -> np.ndarray:
+    ids = np.ascontiguousarray(row_ids, dtype=np.int32)
+    X = np.empty((len(ids), cols), dtype=np.float32)
+    cpu().oracle_fill_rows(X, ids, len(ids), cols, seed, tag, dist)
+    return X
+
+
+def sgemm_basic(A: np.ndarray, B: np.ndarray, C: np.ndarray, alpha: float, beta: float,
+                read_c_if_beta_zero: bool = True, threads: int = 0) -> np.ndarray:
+    """Restatement of kernel_basic; returns a new array (C is not modified)."""
+    m, k = A.shape
+    n = B.shape[1]
+    out = np.ascontiguousarray(C, dtype=np.float32).copy()
+    A = np.ascontiguousarray(A, dtype=np.float32)
+    B = np.ascontiguousarray(B, dtype=np.float32)
+    cpu().oracle_sgemm_basic(m, n, k, alpha, A, max(k, 1), B, max(n, 1), beta, out, max(n, 1),
+                             1 if read_c_if_beta_zero else 0, threads)
+    return out
+
+
+def sgemm_basic_rows(row_ids, A: np.ndarray, B: np.ndarray, C_rows: np.ndarray, alpha: float,
+                     beta: float, read_c_if_beta_zero: bool = True, threads: int = 0) -> np.ndarray:
+    ids = np.ascontiguousarray(row_ids, dtype=np.int32)
+    m, k = A.shape
+    n = B.shape[1]
+    out = np.ascontiguousarray(C_rows, dtype=np.float32).copy()
+    cpu().oracle_sgemm_basic_rows(len(ids), ids, n, k, alpha, np.ascontiguousarray(A), k,
+                                  np.ascontiguousarray(B), n, beta, out, n,
+                                  1 if read_c_if_beta_zero else 0, threads)
+    return out
+
+
+def dgemm(A: np.ndarray, B: np.ndarray, C0: Optional[np.ndarray], alpha: float, beta: float,
+          row_ids=None, threads: int = 0):
+    """FP64 reference and magnitude for all rows (or the listed rows)."""
+    m, k = A.shape
+    n = B.shape[1]
+    ids = None if row_ids is None else np.ascontiguousarray(row_ids, dtype=np.int32)
+    nrows = m if ids is None else len(ids)
+    ref = np.empty((nrows, n), dtype=np.float64)
+    mag = np.empty((nrows, n), dtype=np.float64)
+    c0p = None
+    if C0 is not None:
+        C0 = np.ascontiguousarray(C0, dtype=np.float32)
+        c0p = C0.ctypes.data
+    cpu().oracle_dgemm_rows(nrows, None if ids is None else ids.ctypes.data, n, k, alpha,
+                            np.ascontiguousarray(A, dtype=np.float32), k,
+                            np.ascontiguousarray(B, dtype=np.float32), n, beta, c0p, n, ref,
+                            mag.ctypes.data, threads)
+    return ref, mag
+
+
+def error_stats(C: np.ndarray, ref: np.ndarray, mag: Optional[np.ndarray]) -> dict:
+    out = np.zeros(5, dtype=np.float64)
+    C = np.ascontiguousarray(C, dtype=np.float32)
+    cpu().oracle_error_stats(C.size, C, np.ascontiguousarray(ref, dtype=np.float64),
+                             None if mag is None else np.ascontiguousarray(mag).ctypes.data, out)
+    return {"max_rel": out[0], "mean_rel": out[1], "max_componentwise": out[2],
+            "n_rel": int(out[3]), "non_finite": int(out[4])}
+
+
+# ----------------------------------------------------------------- GPU FP64 --
+
+def gpu() -> ctypes.CDLL:
+    global _gpu
+    if _gpu is None:
+        l = ctypes.CDLL(GPU_LIB)
+        v = ctypes.c_void_p
+        l.oracle_gpu_dgemm.argtypes = [_I, _I, _I, ctypes.c_double, v, _I, v, _I,
+                                       ctypes.c_double, v, _I, v, v]
+        l.oracle_gpu_error_stats.argtypes = [_I, _I, v, _I, v, v, _F64P]
+        _gpu = l
+    return _gpu
+
+
+def gpu_error_stats(A, B, C0, C, alpha: float, beta: float) -> dict:
+    """Full-matrix FP64 error of C (torch CUDA tensors) against alpha*A@B + beta*C0."""
+    import torch
+
+    m, k = A.shape
+    n = B.shape[1]
+    ref = torch.empty((m, n), dtype=torch.float64, device=A.device)
+    mag = torch.empty((m, n), dtype=torch.float64, device=A.device)
+    c0 = C0.data_ptr() if C0 is not None else None
+    assert gpu().oracle_gpu_dgemm(m, n, k, alpha, A.data_ptr(), A.stride(0), B.data_ptr(),
+                                  B.stride(0), beta, c0, n, ref.data_ptr(), mag.data_ptr()) == 0
+    out = np.zeros(5, dtype=np.float64)
+    assert gpu().oracle_gpu_error_stats(m, n, C.data_ptr(), C.stride(0), ref.data_ptr(),
+                                        mag.data_ptr(), out) == 0
+    del ref, mag
+    return {"max_rel": out[0], "mean_rel": out[1], "max_componentwise": out[2],
+            "n_rel": int(out[3]), "non_finite": int(out[4])}
+
+
+# -------------------------------------------------------- reference kernels --
+
+def ref() -> ctypes.CDLL:
+    """The reference's own sgemm()/sgemm_basic(), built from its sources."""
+    global _ref
+    if _ref is None:
+        if not os.path.exists(REF_LIB):
+            raise FileNotFoundError(f"{REF_LIB} not built (make -C oracle with the reference "
+                                    "sources present)")
+        l = ctypes.CDLL(REF_LIB)
+        fp = ctypes.POINTER(ctypes.c_float)
+        v = ctypes.c_void_p
+        for name in ("ref_sgemm", "ref_sgemm_basic"):
+            f = getattr(l, name)
+            f.restype = None
+            f.argtypes = [_I, _I, _I, fp, v, _I, v, _I, fp, v, _I]
+        l.ref_sgemm_kernel_choice.argtypes = [_I, _I]
+        l.ref_sgemm_kernel_choice.restype = _I
+        _ref = l
+    return _ref
+
+
+def ref_sgemm(A, B, C, alpha: float, beta: float, basic: bool = False) -> None:
+    """Run the reference's sgemm() (or sgemm_basic()) on torch CUDA tensors.
+
+    The reference requires ldb == ldc == n (its kernels advance B and C by n);
+    callers pass contiguous tensors.
+    """
+    m, k = A.shape
+    n = B.shape[1]
+    a = ctypes.c_float(alpha)
+    b = ctypes.c_float(beta)
+    f = ref().ref_sgemm_basic if basic else ref().ref_sgemm
+    f(m, n, k, ctypes.byref(a), A.data_ptr(), A.stride(0), B.data_ptr(), B.stride(0),
+      ctypes.byref(b), C.data_ptr(), C.stride(0))

@@ -1,0 +1,75 @@
+// basic.cu — the naive kernel (one thread per C element) and the seeded
+// counter-based generator used by the harnesses.
+//
+// sgemm_b200_basic replaces sgemm_basic()/kernel_basic
+// (src/sgemm.cuh:92-113, src/kernels/basic.cuh:1-26): sequential accumulation
+// acc = fma(A[y,p], B[p,x], acc) for p = 0..k-1, then acc *= alpha and
+// acc = fma(C, beta, acc).  Like the reference it always reads C.
+#include "common.h"
+#include "rng.h"
+
+namespace sgb {
+
+__global__ void basic_kernel(int m, int n, int k, float alpha, const float* __restrict__ A, int lda,
+                             const float* __restrict__ B, int ldb, float beta, float* C, int ldc) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= n || y >= m) return;
+    float acc = 0.0f;
+    for (int p = 0; p < k; ++p) acc = fmaf(A[(int64_t)y * lda + p], B[(int64_t)p * ldb + x], acc);
+    acc = __fmul_rn(acc, alpha);
+    const float c = C[(int64_t)y * ldc + x];
+    C[(int64_t)y * ldc + x] = fmaf(c, beta, acc);
+}
+
+__global__ void fill_kernel(float* X, int rows, int cols, int ld, uint64_t seed, uint32_t tag,
+                            int dist) {
+    const int64_t total = (int64_t)rows * cols;
+    const uint64_t key = rng_key(seed, tag);
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t r = i / cols, c = i % cols;
+        X[r * ld + c] = rng_value(key, static_cast<uint64_t>(i), dist);
+    }
+}
+
+}  // namespace sgb
+
+extern "C" int sgemm_b200_basic(int m, int n, int k, const float* alpha, const float* A, int lda,
+                                const float* B, int ldb, const float* beta, float* C, int ldc,
+                                sgemm_b200_stream_t stream) {
+    int s = sgb::check_gemm_args(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+    if (s == SGEMM_B200_OK && m > 0 && n > 0) {
+        dim3 block(16, 16);
+        dim3 grid(sgb::div_up(n, 16), sgb::div_up(m, 16));
+        sgb::basic_kernel<<<grid, block, 0, sgb::as_stream(stream)>>>(m, n, k, *alpha, A, lda, B,
+                                                                      ldb, *beta, C, ldc);
+        s = sgb::cuda_status(cudaGetLastError());
+    }
+    sgb::set_last_status(s);
+    return s;
+}
+
+extern "C" void sgemm_basic(int m, int n, int k, const float* alpha, float* A, int lda, float* B,
+                            int ldb, const float* beta, float* C, int ldc) {
+    sgemm_b200_basic(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, nullptr);
+}
+
+extern "C" int sgemm_b200_fill_random(float* X, int rows, int cols, int ld, uint64_t seed,
+                                      uint32_t tag, int dist, sgemm_b200_stream_t stream) {
+    if (rows < 0 || cols < 0 || ld < cols || dist < 0 || dist > 2) {
+        sgb::set_last_status(SGEMM_B200_ERR_INVALID_ARG);
+        return SGEMM_B200_ERR_INVALID_ARG;
+    }
+    if (rows == 0 || cols == 0) return SGEMM_B200_OK;
+    if (!X) return SGEMM_B200_ERR_INVALID_ARG;
+    const int64_t total = (int64_t)rows * cols;
+    const int threads = 256;
+    int64_t blocks = (total + threads - 1) / threads;
+    if (blocks > 148 * 64) blocks = 148 * 64;
+    sgb::fill_kernel<<<(int)blocks, threads, 0, sgb::as_stream(stream)>>>(X, rows, cols, ld, seed,
+                                                                          tag, dist);
+    int s = sgb::cuda_status(cudaGetLastError());
+    sgb::set_last_status(s);
+    return s;
+}

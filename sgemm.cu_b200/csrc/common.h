@@ -1,0 +1,55 @@
+// common.h — host-side helpers shared by every translation unit of the library.
+#pragma once
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+
+#include "../../include/sgemm_b200.h"
+
+namespace sgb {
+
+// Per-thread status of the most recent public call (sgemm() returns void,
+// like the reference, so its outcome is kept here).
+void set_last_status(int s);
+
+// Device address of the library's status word (bounded waits write
+// SGEMM_B200_ERR_TIMEOUT there).  Resolved once per device.
+int* device_status_ptr();
+
+// Cached properties of the current device.
+struct DeviceInfo {
+    int device = -1;
+    int sm_count = 0;
+    int cc_major = 0, cc_minor = 0;
+    size_t smem_optin = 0;
+    char name[256] = {0};
+};
+const DeviceInfo& device_info();
+
+// True when the current device can run sm_100a code.
+bool device_is_sm100();
+
+inline cudaStream_t as_stream(sgemm_b200_stream_t s) { return reinterpret_cast<cudaStream_t>(s); }
+
+inline int cuda_status(cudaError_t e) {
+    if (e == cudaSuccess) return SGEMM_B200_OK;
+    if (e == cudaErrorMemoryAllocation) return SGEMM_B200_ERR_NO_MEMORY;
+    return SGEMM_B200_ERR_CUDA;
+}
+
+// Tensor-map encoding through the driver entry point (no link against libcuda).
+bool encode_tensor_map_2d(CUtensorMap* map, CUtensorMapDataType dtype, const void* base,
+                          uint64_t inner_elems, uint64_t outer_elems, uint64_t row_stride_bytes,
+                          uint32_t box_inner, uint32_t box_outer, CUtensorMapSwizzle swizzle);
+
+// Shape checks common to every entry point.  Returns SGEMM_B200_OK or
+// SGEMM_B200_ERR_INVALID_ARG.
+int check_gemm_args(int m, int n, int k, const float* alpha, const void* A, int lda,
+                    const void* B, int ldb, const float* beta, const void* C, int ldc);
+
+inline int div_up(int a, int b) { return (a + b - 1) / b; }
+
+}  // namespace sgb

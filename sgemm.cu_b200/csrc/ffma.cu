@@ -1,0 +1,196 @@
+// ffma.cu — plain-path kernel configurations, dispatch and the C ABI entry
+// points that replace the reference's sgemm() (src/sgemm.cuh:19-48).
+#include <cmath>
+#include <cstring>
+#include <mutex>
+
+#include "common.h"
+#include "ffma_kernel.cuh"
+#include "plain.h"
+
+namespace sgb {
+namespace ffma {
+
+// Compiled configurations.  Index = public config id.
+//   name                 tile      warps  thread tile  stages  loader
+using C0 = Cfg<128, 256, 4, 2, 16, 4, kLoaderTma, 1>;     // 192 KB smem, 1 CTA/SM
+using C1 = Cfg<128, 128, 4, 2, 8, 3, kLoaderTma, 2>;      //  96 KB, 2 CTAs/SM
+using C2 = Cfg<64, 128, 2, 2, 8, 4, kLoaderTma, 2>;       //  96 KB, 2 CTAs/SM
+using C3 = Cfg<64, 64, 2, 1, 8, 4, kLoaderTma, 3>;        //  64 KB, 3 CTAs/SM
+using C4 = Cfg<128, 256, 4, 2, 16, 4, kLoaderAsync4, 1>;
+using C5 = Cfg<128, 128, 4, 2, 8, 3, kLoaderAsync4, 2>;
+using C6 = Cfg<64, 128, 2, 2, 8, 4, kLoaderAsync4, 2>;
+using C7 = Cfg<64, 64, 2, 1, 8, 4, kLoaderAsync4, 3>;
+
+struct ConfigDesc {
+    const char* name;
+    int bm, bn, threads, smem, loader;
+    float efficiency;  // relative per-SM FFMA efficiency used by the dispatcher
+    void (*kernel)(const CUtensorMap, const CUtensorMap, const Params);
+};
+
+template <class C>
+constexpr ConfigDesc describe(const char* name, float eff) {
+    return ConfigDesc{name, C::BM, C::BN, C::THREADS, C::SMEM_BYTES, C::LOADER, eff,
+                      &ffma_gemm_kernel<C>};
+}
+
+static const ConfigDesc kConfigs[] = {
+    describe<C0>("tma_128x256_t8x16_s4", 1.00f),  describe<C1>("tma_128x128_t8x8_s3", 0.92f),
+    describe<C2>("tma_64x128_t8x8_s4", 0.88f),    describe<C3>("tma_64x64_t8x8_s4", 0.80f),
+    describe<C4>("cpa_128x256_t8x16_s4", 0.97f),  describe<C5>("cpa_128x128_t8x8_s3", 0.90f),
+    describe<C6>("cpa_64x128_t8x8_s4", 0.85f),    describe<C7>("cpa_64x64_t8x8_s4", 0.78f),
+};
+constexpr int kNumConfigs = sizeof(kConfigs) / sizeof(kConfigs[0]);
+constexpr int kNumPerLoader = kNumConfigs / 2;
+
+static int occupancy(int cfg) {
+    static int occ[64][kNumConfigs];
+    static bool have[64][kNumConfigs];
+    static std::mutex mu;
+    const DeviceInfo& d = device_info();
+    if (d.device < 0 || d.device >= 64) return 1;
+    std::lock_guard<std::mutex> lock(mu);
+    if (!have[d.device][cfg]) {
+        const ConfigDesc& c = kConfigs[cfg];
+        int o = 0;
+        cudaFuncSetAttribute(c.kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, c.smem);
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, c.kernel, c.threads, c.smem) !=
+                cudaSuccess ||
+            o < 1)
+            o = 1;
+        occ[d.device][cfg] = o;
+        have[d.device][cfg] = true;
+    }
+    return occ[d.device][cfg];
+}
+
+static bool tma_ok(const float* A, int lda, const float* B, int ldb) {
+    return (lda % 4 == 0) && (ldb % 4 == 0) && (reinterpret_cast<uintptr_t>(A) % 16 == 0) &&
+           (reinterpret_cast<uintptr_t>(B) % 16 == 0);
+}
+
+}  // namespace ffma
+
+int plain_config_count() { return ffma::kNumConfigs; }
+const char* plain_config_name(int cfg) {
+    return (cfg >= 0 && cfg < ffma::kNumConfigs) ? ffma::kConfigs[cfg].name : nullptr;
+}
+int plain_config_tile(int cfg, int* bm, int* bn) {
+    if (cfg < 0 || cfg >= ffma::kNumConfigs) return SGEMM_B200_ERR_INVALID_ARG;
+    *bm = ffma::kConfigs[cfg].bm;
+    *bn = ffma::kConfigs[cfg].bn;
+    return SGEMM_B200_OK;
+}
+
+// Pick the configuration with the smallest modelled time:
+//   waves(cfg) * tile_work(cfg) / efficiency(cfg)
+// where waves = ceil(tiles / (SMs * resident CTAs per SM)).
+int plain_select(int m, int n, int k, const float* A, int lda, const float* B, int ldb) {
+    using namespace ffma;
+    const int base = (k == 0 || tma_ok(A, lda, B, ldb)) ? 0 : kNumPerLoader;
+    const DeviceInfo& d = device_info();
+    const int sms = d.sm_count > 0 ? d.sm_count : 148;
+    int best = base;
+    double best_t = 1e300;
+    for (int c = base; c < base + kNumPerLoader; ++c) {
+        const ConfigDesc& cd = kConfigs[c];
+        const double tiles = double(div_up(m, cd.bm)) * div_up(n, cd.bn);
+        const double slots = double(sms) * occupancy(c);
+        const double waves = std::ceil(tiles / slots);
+        // Work per tile, with its resident-CTA share of the SM.
+        const double t = waves * double(cd.bm) * cd.bn / (cd.efficiency * occupancy(c));
+        if (t < best_t * 0.999) {
+            best_t = t;
+            best = c;
+        }
+    }
+    (void)k;
+    return best;
+}
+
+int plain_launch(int cfg, int m, int n, int k, float alpha, const float* A, int lda,
+                 const float* B, int ldb, float beta, float* C, int ldc, cudaStream_t stream) {
+    using namespace ffma;
+    if (m == 0 || n == 0) return SGEMM_B200_OK;
+    if (!device_is_sm100()) return SGEMM_B200_ERR_UNSUPPORTED;
+    if (cfg < 0) cfg = plain_select(m, n, k, A, lda, B, ldb);
+    if (cfg >= kNumConfigs) return SGEMM_B200_ERR_INVALID_ARG;
+    const ConfigDesc& cd = kConfigs[cfg];
+    if (cd.loader == kLoaderTma && k > 0 && !tma_ok(A, lda, B, ldb))
+        return SGEMM_B200_ERR_INVALID_ARG;
+
+    Params p;
+    p.m = m;
+    p.n = n;
+    p.k = k;
+    p.lda = lda;
+    p.ldb = ldb;
+    p.ldc = ldc;
+    p.alpha = alpha;
+    p.beta = beta;
+    p.A = A;
+    p.B = B;
+    p.C = C;
+    p.status = device_status_ptr();
+    if (!p.status) return SGEMM_B200_ERR_CUDA;
+    p.tiles_m = div_up(m, cd.bm);
+    p.tiles_n = div_up(n, cd.bn);
+    p.vec_c = (ldc % 4 == 0) && (reinterpret_cast<uintptr_t>(C) % 16 == 0);
+
+    CUtensorMap tmA, tmB;
+    std::memset(&tmA, 0, sizeof(tmA));
+    std::memset(&tmB, 0, sizeof(tmB));
+    if (cd.loader == kLoaderTma && k > 0) {
+        if (!encode_tensor_map_2d(&tmA, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, A, (uint64_t)k,
+                                  (uint64_t)m, (uint64_t)lda * 4, 32, cd.bm,
+                                  CU_TENSOR_MAP_SWIZZLE_128B) ||
+            !encode_tensor_map_2d(&tmB, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, B, (uint64_t)n,
+                                  (uint64_t)k, (uint64_t)ldb * 4, cd.bn, 32,
+                                  CU_TENSOR_MAP_SWIZZLE_NONE))
+            return SGEMM_B200_ERR_CUDA;
+    }
+    occupancy(cfg);  // sets the dynamic shared-memory attribute once per device
+    const int grid = p.tiles_m * p.tiles_n;
+    cd.kernel<<<grid, cd.threads, cd.smem, stream>>>(tmA, tmB, p);
+    return cuda_status(cudaGetLastError());
+}
+
+}  // namespace sgb
+
+// ---------------------------------------------------------------- C ABI --
+
+extern "C" int sgemm_b200_with_config(int cfg, int m, int n, int k, const float* alpha,
+                                      const float* A, int lda, const float* B, int ldb,
+                                      const float* beta, float* C, int ldc,
+                                      sgemm_b200_stream_t stream) {
+    int s = sgb::check_gemm_args(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+    if (s == SGEMM_B200_OK)
+        s = sgb::plain_launch(cfg, m, n, k, *alpha, A, lda, B, ldb, *beta, C, ldc,
+                              sgb::as_stream(stream));
+    sgb::set_last_status(s);
+    return s;
+}
+
+extern "C" int sgemm_b200(int m, int n, int k, const float* alpha, const float* A, int lda,
+                          const float* B, int ldb, const float* beta, float* C, int ldc,
+                          sgemm_b200_stream_t stream) {
+    return sgemm_b200_with_config(-1, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, stream);
+}
+
+extern "C" void sgemm(int m, int n, int k, const float* alpha, float* A, int lda, float* B,
+                      int ldb, const float* beta, float* C, int ldc) {
+    sgemm_b200(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, nullptr);
+}
+
+extern "C" int sgemm_b200_config_count(void) { return sgb::plain_config_count(); }
+
+extern "C" const char* sgemm_b200_config_name(int cfg) { return sgb::plain_config_name(cfg); }
+
+extern "C" int sgemm_b200_select_config(int m, int n, int k, const float* A, int lda,
+                                        const float* B, int ldb, const float* C, int ldc) {
+    (void)C;
+    (void)ldc;
+    if (m <= 0 || n <= 0 || k < 0) return -1;
+    return sgb::plain_select(m, n, k, A, lda, B, ldb);
+}

@@ -1,0 +1,284 @@
+// ffma_kernel.cuh — the plain FP32 path: register-blocked FFMA SGEMM for sm_100a.
+//
+// Replaces the reference's sgemm_128x128x8 / sgemm_128x256x8
+// (src/kernels/128x128x8.cuh, src/kernels/128x256x8.cuh).  Same contract and
+// same arithmetic per C element:
+//     acc = 0; for p = 0..k-1 in increasing order: acc = fma(A[i,p], B[p,j], acc)
+//     acc = acc * alpha;  C[i,j] = beta != 0 ? fma(C[i,j], beta, acc) : acc
+// (reference: 128x256x8.cuh:224-239 for the chain, :331-337 for alpha,
+// :365-380 for the beta branch), so outputs are bit-identical.  Zero-filled
+// k padding adds exact +0 terms, as the reference's padded first block does
+// (128x256x8.cuh:87-116).
+//
+// B200 design (not the reference's):
+//  - CTA tile BM x BN with a 32-deep k block, STAGES-deep ring of stages in
+//    shared memory filled by TMA (one elected thread, mbarrier completion) or,
+//    for strides that TMA cannot describe (lda/ldb not a multiple of 4),
+//    by 4-byte cp.async with zero fill;
+//  - A is kept k-contiguous ([m][32] rows of 128 B) with the 128-byte XOR
+//    swizzle TMA applies, so a thread reads 4 k-values of one row with one
+//    conflict-free 128-bit shared load (instead of transposing A in smem);
+//  - B is kept [32][BN]; each 128-bit load is broadcast to the 4 lanes that
+//    share a column group (warp-level operand broadcast);
+//  - thread tile 8 (m) x TN (n); lanes 4 (m) x 8 (n); warps WM x WN;
+//  - epilogue straight from registers with float4 stores: for a fixed
+//    register group a warp writes 4 rows x 128 contiguous bytes.
+#pragma once
+
+#include <cstdint>
+
+#include "ptx.cuh"
+
+namespace sgb {
+namespace ffma {
+
+enum Loader { kLoaderTma = 0, kLoaderAsync4 = 1 };
+
+template <int BM_, int BN_, int WM_, int WN_, int TN_, int STAGES_, int LOADER_, int MINB_ = 1>
+struct Cfg {
+    static constexpr int BM = BM_, BN = BN_, WM = WM_, WN = WN_, TN = TN_, STAGES = STAGES_;
+    static constexpr int LOADER = LOADER_;
+    static constexpr int MINB = MINB_;  // resident CTAs per SM the register budget targets
+    static constexpr int BK = 32;  // one 128-byte row of A per k block
+    static constexpr int TM = 8;
+    static constexpr int THREADS = 32 * WM * WN;
+    static_assert(BM == WM * 4 * TM, "4 lanes x 8 rows per warp along m");
+    static_assert(BN == WN * 8 * TN, "8 lanes x TN columns per warp along n");
+    static_assert(TN % 4 == 0, "columns come in float4 groups");
+    static constexpr int A_BYTES = BM * BK * 4;
+    static constexpr int B_BYTES = BK * BN * 4;
+    static constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
+    static_assert(A_BYTES % 1024 == 0 && STAGE_BYTES % 1024 == 0, "1024-byte swizzle atoms");
+    static constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024;  // + alignment slack
+};
+
+struct Params {
+    int m, n, k;
+    int lda, ldb, ldc;
+    float alpha, beta;
+    const float* A;
+    const float* B;
+    float* C;
+    int* status;
+    int tiles_m, tiles_n;
+    int vec_c;  // C rows are 16-byte aligned (ldc % 4 == 0 and C aligned)
+};
+
+// Grouped rasterisation: 8 tile-rows share a band so concurrently resident
+// CTAs reuse A rows and B columns out of L2.
+__device__ __forceinline__ void tile_coords(int bid, int tiles_m, int tiles_n, int& tm, int& tn) {
+    constexpr int G = 8;
+    const int per_group = G * tiles_n;
+    const int gid = bid / per_group;
+    const int first = gid * G;
+    const int gsz = min(tiles_m - first, G);
+    const int r = bid % per_group;
+    tm = first + r % gsz;
+    tn = r / gsz;
+}
+
+// Accumulate one 32-deep k block held in shared memory.
+template <class C>
+__device__ __forceinline__ void compute_stage(const uint8_t* __restrict__ As,
+                                              const uint8_t* __restrict__ Bs, uint32_t a_base,
+                                              uint32_t xa0, uint32_t xa1, uint32_t b_base,
+                                              float (&acc)[C::TM][C::TN]) {
+#pragma unroll
+    for (int k4 = 0; k4 < C::BK / 4; ++k4) {
+        float4 a[C::TM];
+#pragma unroll
+        for (int i = 0; i < C::TM; ++i) {
+            const uint32_t x = (i & 1) ? xa1 : xa0;
+            const uint32_t off = a_base + i * 4 * 128 + ((static_cast<uint32_t>(k4) << 4) ^ x);
+            a[i] = *reinterpret_cast<const float4*>(As + off);
+        }
+#pragma unroll
+        for (int kk = 0; kk < 4; ++kk) {
+            float4 b[C::TN / 4];
+#pragma unroll
+            for (int g = 0; g < C::TN / 4; ++g)
+                b[g] = *reinterpret_cast<const float4*>(Bs + (k4 * 4 + kk) * C::BN * 4 + b_base +
+                                                        g * 128);
+#pragma unroll
+            for (int i = 0; i < C::TM; ++i) {
+                const float av = kk == 0 ? a[i].x : kk == 1 ? a[i].y : kk == 2 ? a[i].z : a[i].w;
+#pragma unroll
+                for (int g = 0; g < C::TN / 4; ++g) {
+                    acc[i][4 * g + 0] = fmaf(av, b[g].x, acc[i][4 * g + 0]);
+                    acc[i][4 * g + 1] = fmaf(av, b[g].y, acc[i][4 * g + 1]);
+                    acc[i][4 * g + 2] = fmaf(av, b[g].z, acc[i][4 * g + 2]);
+                    acc[i][4 * g + 3] = fmaf(av, b[g].w, acc[i][4 * g + 3]);
+                }
+            }
+        }
+    }
+}
+
+// cp.async loader for one k block (any stride, any alignment).
+template <class C>
+__device__ __forceinline__ void load_stage_async4(const Params& p, uint8_t* As, uint8_t* Bs, int m0,
+                                                  int n0, int k0, int tid) {
+    const uint32_t as = smem_u32(As), bs = smem_u32(Bs);
+    constexpr int A_ELEMS = C::BM * C::BK;
+#pragma unroll 4
+    for (int e = tid; e < A_ELEMS; e += C::THREADS) {
+        const int r = e >> 5, c = e & 31;
+        const bool ok = (m0 + r < p.m) && (k0 + c < p.k);
+        const float* src = ok ? p.A + (int64_t)(m0 + r) * p.lda + (k0 + c) : p.A;
+        const uint32_t dst = as + r * 128 + ((((c >> 2) ^ (r & 7)) << 4) | ((c & 3) << 2));
+        cp_async_4_zfill(dst, src, ok);
+    }
+    constexpr int B_ELEMS = C::BK * C::BN;
+#pragma unroll 4
+    for (int e = tid; e < B_ELEMS; e += C::THREADS) {
+        const int r = e / C::BN, c = e % C::BN;
+        const bool ok = (k0 + r < p.k) && (n0 + c < p.n);
+        const float* src = ok ? p.B + (int64_t)(k0 + r) * p.ldb + (n0 + c) : p.B;
+        cp_async_4_zfill(bs + (r * C::BN + c) * 4, src, ok);
+    }
+}
+
+template <class C>
+__device__ __forceinline__ void epilogue(const Params& p, int m0, int n0, int wm, int wn, int lm,
+                                         int ln, float (&acc)[C::TM][C::TN]) {
+    const int col0 = n0 + wn * 8 * C::TN + ln * 4;
+#pragma unroll
+    for (int i = 0; i < C::TM; ++i) {
+        const int row = m0 + wm * 32 + lm + 4 * i;
+        if (row >= p.m) continue;
+        float* crow = p.C + (int64_t)row * p.ldc;
+#pragma unroll
+        for (int g = 0; g < C::TN / 4; ++g) {
+            const int col = col0 + 32 * g;
+            float v[4];
+#pragma unroll
+            for (int e = 0; e < 4; ++e) v[e] = __fmul_rn(acc[i][4 * g + e], p.alpha);
+            if (p.vec_c && col + 3 < p.n) {
+                float4* dst = reinterpret_cast<float4*>(crow + col);
+                if (p.beta != 0.0f) {
+                    const float4 o = *dst;
+                    v[0] = fmaf(o.x, p.beta, v[0]);
+                    v[1] = fmaf(o.y, p.beta, v[1]);
+                    v[2] = fmaf(o.z, p.beta, v[2]);
+                    v[3] = fmaf(o.w, p.beta, v[3]);
+                }
+                *dst = make_float4(v[0], v[1], v[2], v[3]);
+            } else {
+#pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                    if (col + e < p.n) {
+                        float out = v[e];
+                        if (p.beta != 0.0f) out = fmaf(crow[col + e], p.beta, out);
+                        crow[col + e] = out;
+                    }
+                }
+            }
+        }
+    }
+}
+
+template <class C>
+__global__ void __launch_bounds__(C::THREADS, C::MINB)
+    ffma_gemm_kernel(const __grid_constant__ CUtensorMap tmA,
+                     const __grid_constant__ CUtensorMap tmB, const Params p) {
+    extern __shared__ uint8_t smem_raw[];
+    __shared__ __align__(8) uint64_t full_bar[C::STAGES];
+    uint8_t* smem = reinterpret_cast<uint8_t*>(
+        (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
+
+    const int tid = threadIdx.x;
+    const int warp = tid >> 5, lane = tid & 31;
+    const int wm = warp / C::WN, wn = warp % C::WN;
+    const int lm = lane >> 3, ln = lane & 7;
+
+    int tm, tn;
+    tile_coords(blockIdx.x, p.tiles_m, p.tiles_n, tm, tn);
+    const int m0 = tm * C::BM, n0 = tn * C::BN;
+    const int nk = (p.k + C::BK - 1) / C::BK;
+
+    // Per-thread shared-memory offsets (bytes within a stage).
+    const uint32_t a_base = static_cast<uint32_t>((wm * 32 + lm) * 128);
+    const uint32_t xa0 = static_cast<uint32_t>(lm) << 4;        // row % 8 for even i
+    const uint32_t xa1 = static_cast<uint32_t>(lm + 4) << 4;    // row % 8 for odd i
+    const uint32_t b_base = static_cast<uint32_t>((wn * 8 * C::TN + ln * 4) * 4);
+
+    float acc[C::TM][C::TN];
+#pragma unroll
+    for (int i = 0; i < C::TM; ++i)
+#pragma unroll
+        for (int j = 0; j < C::TN; ++j) acc[i][j] = 0.0f;
+
+    if constexpr (C::LOADER == kLoaderTma) {
+        int issued = 0;
+        auto issue = [&](int kb) {
+            const int s = kb % C::STAGES;
+            uint8_t* st = smem + s * C::STAGE_BYTES;
+            mbar_arrive_expect_tx(&full_bar[s], C::STAGE_BYTES);
+            tma_load_2d(st, &tmA, &full_bar[s], kb * C::BK, m0);
+            tma_load_2d(st + C::A_BYTES, &tmB, &full_bar[s], n0, kb * C::BK);
+        };
+        if (tid == 0) {
+            for (int s = 0; s < C::STAGES; ++s) mbar_init(&full_bar[s], 1);
+            fence_barrier_init();
+            if (nk > 0) {
+                tma_prefetch_desc(&tmA);
+                tma_prefetch_desc(&tmB);
+            }
+        }
+        __syncthreads();
+        if (tid == 0) {
+            for (; issued < C::STAGES && issued < nk; ++issued) issue(issued);
+        }
+        int kb = 0;
+        bool failed = false;
+        for (; kb < nk; ++kb) {
+            const int s = kb % C::STAGES;
+            const bool ok = mbar_wait(&full_bar[s], (kb / C::STAGES) & 1);
+            if (__syncthreads_or(!ok)) {
+                failed = true;
+                break;
+            }
+            // Every thread finished block kb-1, so its stage ((kb-1) % STAGES,
+            // which is where block kb-1+STAGES == issued lands) may be refilled.
+            if (tid == 0 && kb > 0 && issued < nk) issue(issued++);
+            const uint8_t* st = smem + s * C::STAGE_BYTES;
+            compute_stage<C>(st, st + C::A_BYTES, a_base, xa0, xa1, b_base, acc);
+        }
+        if (failed) {
+            if (tid == 0) {
+                atomicExch(p.status, SGEMM_B200_ERR_TIMEOUT);
+                // Let copies still in flight land before the CTA's smem is released.
+                for (int j = kb; j < issued; ++j)
+                    if (!mbar_wait(&full_bar[j % C::STAGES], (j / C::STAGES) & 1)) break;
+            }
+            return;
+        }
+    } else {
+#pragma unroll
+        for (int s = 0; s < C::STAGES - 1; ++s) {
+            if (s < nk) {
+                uint8_t* st = smem + s * C::STAGE_BYTES;
+                load_stage_async4<C>(p, st, st + C::A_BYTES, m0, n0, s * C::BK, tid);
+            }
+            cp_async_commit();
+        }
+        for (int kb = 0; kb < nk; ++kb) {
+            cp_async_wait<C::STAGES - 2>();
+            __syncthreads();
+            const int nxt = kb + C::STAGES - 1;
+            if (nxt < nk) {
+                uint8_t* st = smem + (nxt % C::STAGES) * C::STAGE_BYTES;
+                load_stage_async4<C>(p, st, st + C::A_BYTES, m0, n0, nxt * C::BK, tid);
+            }
+            cp_async_commit();
+            const uint8_t* st = smem + (kb % C::STAGES) * C::STAGE_BYTES;
+            compute_stage<C>(st, st + C::A_BYTES, a_base, xa0, xa1, b_base, acc);
+        }
+        cp_async_wait<0>();
+    }
+
+    epilogue<C>(p, m0, n0, wm, wn, lm, ln, acc);
+}
+
+}  // namespace ffma
+}  // namespace sgb

@@ -1,0 +1,16 @@
+// plain.h — internal interface of the plain FFMA path (used by the grouped
+// kernel's sequential baseline, the autotuner and the serving loop).
+#pragma once
+
+#include <cuda_runtime.h>
+
+namespace sgb {
+
+int plain_config_count();
+const char* plain_config_name(int cfg);
+int plain_config_tile(int cfg, int* bm, int* bn);
+int plain_select(int m, int n, int k, const float* A, int lda, const float* B, int ldb);
+int plain_launch(int cfg, int m, int n, int k, float alpha, const float* A, int lda,
+                 const float* B, int ldb, float beta, float* C, int ldc, cudaStream_t stream);
+
+}  // namespace sgb

@@ -1,0 +1,81 @@
+// test_sgemm.cu — correctness sweep through the public API, the reference's
+// test lane (test.cu:18-121, test.sh:1-13) rebuilt on this library.
+//
+// For every square size mmin..mmax (step mstep): seeded inputs, one call of
+// the chosen path, one call of the naive kernel (sgemm_b200_basic, the
+// reference's sgemm_basic), then the reference's comparison (relative error
+// <= 1e-4, NaN/Inf are failures).  Differences from the reference harness:
+// reproducible seeded inputs instead of srand(time(NULL)); the plain path is
+// also checked for bit-exact equality; the exit status is non-zero when any
+// size fails (the reference always exits 0, test.cu:120).
+//
+//   bin/test_sgemm --mmin=2 --mmax=3072 --mstep=1 --savedir=test_results
+//                  [--path=plain|bf16x6|tf32x3] [--seed=0] [--dist=u01|upm1|pow2]
+#include <filesystem>
+#include <fstream>
+
+#include "harness_common.h"
+
+int main(int argc, char** argv) {
+    using namespace harness;
+    const int mmax = flag_int(argc, argv, "mmax", 1024);
+    const int mmin = flag_int(argc, argv, "mmin", 2);
+    const int mstep = std::max(1, flag_int(argc, argv, "mstep", 1));
+    const std::string savedir = flag_str(argc, argv, "savedir", "test_results");
+    const int path = parse_path(flag_str(argc, argv, "path", "plain"));
+    const int dist = parse_dist(flag_str(argc, argv, "dist", "u01"));
+    const uint64_t seed = (uint64_t)flag_int(argc, argv, "seed", 0);
+    const float alpha = (float)flag_double(argc, argv, "alpha", 1.5);
+    const float beta = (float)flag_double(argc, argv, "beta", 0.5);
+
+    std::printf("=========================\nTesting...\n=========================\n");
+    const int n_tests = (mmax - mmin) / mstep + 1;
+    int n_failed = 0;
+    std::string failed, full;
+    for (int t = 0; t < n_tests; ++t) {
+        const int s = mmin + t * mstep;
+        const int m = s, n = s, k = s, lda = k, ldb = n, ldc = n;
+        float *A, *B, *C, *Cref;
+        HCHECK(cudaMalloc(&A, sizeof(float) * (size_t)m * lda));
+        HCHECK(cudaMalloc(&B, sizeof(float) * (size_t)k * ldb));
+        HCHECK(cudaMalloc(&C, sizeof(float) * (size_t)m * ldc));
+        HCHECK(cudaMalloc(&Cref, sizeof(float) * (size_t)m * ldc));
+        SCHECK(sgemm_b200_fill_random(A, m, k, lda, seed, 1, dist, nullptr));
+        SCHECK(sgemm_b200_fill_random(B, k, n, ldb, seed, 2, dist, nullptr));
+        SCHECK(sgemm_b200_fill_random(C, m, n, ldc, seed, 3, dist, nullptr));
+        HCHECK(cudaMemcpy(Cref, C, sizeof(float) * (size_t)m * ldc, cudaMemcpyDeviceToDevice));
+        SCHECK(sgemm_b200_gemm(path, m, n, k, &alpha, A, lda, B, ldb, &beta, C, ldc, nullptr));
+        SCHECK(sgemm_b200_basic(m, n, k, &alpha, A, lda, B, ldb, &beta, Cref, ldc, nullptr));
+        std::vector<float> hc((size_t)m * ldc), hr((size_t)m * ldc);
+        HCHECK(cudaMemcpy(hc.data(), C, sizeof(float) * hc.size(), cudaMemcpyDeviceToHost));
+        HCHECK(cudaMemcpy(hr.data(), Cref, sizeof(float) * hr.size(), cudaMemcpyDeviceToHost));
+        HCHECK(cudaGetLastError());
+        CmpResult r = compare_mats(hr.data(), hc.data(), hc.size(), 1e-4f);
+        const bool exact_ok = path != SGEMM_B200_PATH_PLAIN || r.n_bit_exact == (long)hc.size();
+        const bool ok = r.equal && exact_ok;
+        if (!ok) {
+            ++n_failed;
+            failed += std::to_string(t) + " ";
+        }
+        std::printf("Test #%i | matsize = %i | %s | bit-exact %ld/%zu\n", t, s,
+                    ok ? "PASSED" : "FAILED", r.n_bit_exact, hc.size());
+        full += "Test #" + std::to_string(t) + " Matsize = " + std::to_string(s) +
+                ": n_false = " + std::to_string(r.n_false) + ", n_nan = " +
+                std::to_string(r.n_nan) + ", n_inf = " + std::to_string(r.n_inf) +
+                ", bit_exact = " + std::to_string(r.n_bit_exact) + "\n";
+        HCHECK(cudaFree(A));
+        HCHECK(cudaFree(B));
+        HCHECK(cudaFree(C));
+        HCHECK(cudaFree(Cref));
+    }
+    std::string summary = "\n=============== SUMMARY ===============\nPASSED: " +
+                          std::to_string(n_tests - n_failed) + " / " + std::to_string(n_tests) +
+                          "\nFAILED: " + (failed.empty() ? std::string("0") : failed) + "\n";
+    std::printf("%s", summary.c_str());
+    std::filesystem::create_directories(savedir);
+    const std::string out = savedir + "/sgemm.cu.txt";
+    std::ofstream f(out);
+    f << full << summary;
+    std::printf("Test results stored in %s\n", out.c_str());
+    return n_failed == 0 ? 0 : 1;
+}

@@ -1,0 +1,265 @@
+"""Python binding of libsgemm_b200.so (ctypes over the C ABI in include/sgemm_b200.h).
+
+The binding is the host-side mirror the Python tests and the benchmark use: it
+passes torch CUDA tensors' device pointers straight to the C ABI.  PyTorch is
+only the device-memory and stream plumbing; every GEMM runs in the library's
+own sm_100a kernels.  There is no fallback: if the shared library is missing
+or the device is not sm_100, calls raise.
+
+Reference mapping (szrlee/sgemm.cu):
+  sgemm()        -> src/sgemm.cuh:19-90   (plain FFMA path, bit-exact)
+  sgemm_basic()  -> src/sgemm.cuh:92-113  (naive one-thread-per-element kernel)
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Optional, Sequence
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "lib", "libsgemm_b200.so")
+
+OK = 0
+ERR_INVALID_ARG = 1
+ERR_UNSUPPORTED = 2
+ERR_CUDA = 3
+ERR_TIMEOUT = 4
+ERR_NO_MEMORY = 5
+ERR_REJECTED = 6
+
+PATH_PLAIN = 0
+PATH_BF16X6 = 1
+PATH_TF32X3 = 2
+PATHS = {"plain": PATH_PLAIN, "bf16x6": PATH_BF16X6, "tf32x3": PATH_TF32X3}
+
+DIST_UNIFORM_PM1 = 0
+DIST_UNIFORM_01 = 1
+DIST_SIGNED_POW2 = 2
+
+
+class SgemmError(RuntimeError):
+    def __init__(self, status: int, what: str = ""):
+        self.status = status
+        msg = status_string(status) if _lib is not None else str(status)
+        super().__init__(f"{what}: {msg} (status {status})" if what else msg)
+
+
+class Problem(ctypes.Structure):
+    """Mirror of sgemm_b200_problem."""
+
+    _fields_ = [
+        ("m", ctypes.c_int), ("n", ctypes.c_int), ("k", ctypes.c_int),
+        ("lda", ctypes.c_int), ("ldb", ctypes.c_int), ("ldc", ctypes.c_int),
+        ("alpha", ctypes.c_float), ("beta", ctypes.c_float),
+        ("A", ctypes.c_void_p), ("B", ctypes.c_void_p), ("C", ctypes.c_void_p),
+    ]
+
+
+_lib: Optional[ctypes.CDLL] = None
+
+_I = ctypes.c_int
+_P = ctypes.c_void_p
+_FP = ctypes.POINTER(ctypes.c_float)
+_GEMM_ARGS = [_I, _I, _I, _FP, _P, _I, _P, _I, _FP, _P, _I]
+
+
+def _declare(lib: ctypes.CDLL) -> None:
+    def d(name, res, args):
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+
+    d("sgemm_b200", _I, _GEMM_ARGS + [_P])
+    d("sgemm_b200_with_config", _I, [_I] + _GEMM_ARGS + [_P])
+    d("sgemm_b200_config_count", _I, [])
+    d("sgemm_b200_config_name", ctypes.c_char_p, [_I])
+    d("sgemm_b200_select_config", _I, [_I, _I, _I, _P, _I, _P, _I, _P, _I])
+    d("sgemm_b200_basic", _I, _GEMM_ARGS + [_P])
+    d("sgemm_b200_split_workspace_size", ctypes.c_size_t, [_I, _I, _I, _I])
+    d("sgemm_b200_split", _I, [_I] + _GEMM_ARGS + [_P, ctypes.c_size_t, _P])
+    d("sgemm_b200_gemm", _I, [_I] + _GEMM_ARGS + [_P])
+    d("sgemm_b200_grouped_plan_create", _I,
+      [ctypes.POINTER(_P), ctypes.POINTER(Problem), _I, ctypes.c_char_p])
+    d("sgemm_b200_grouped_plan_launch", _I, [_P, _P, _I])
+    d("sgemm_b200_grouped_plan_info", _I,
+      [_P, ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(_I)])
+    d("sgemm_b200_grouped_plan_destroy", None, [_P])
+    d("sgemm_b200_grouped", _I, [ctypes.POINTER(Problem), _I, _P])
+    d("sgemm_b200_autotune_grouped", _I, [ctypes.POINTER(Problem), _I, ctypes.c_char_p])
+    d("sgemm_b200_fill_random", _I, [_P, _I, _I, _I, ctypes.c_uint64, ctypes.c_uint32, _I, _P])
+    d("sgemm_b200_device_status", _I, [])
+    d("sgemm_b200_last_status", _I, [])
+    d("sgemm_b200_status_string", ctypes.c_char_p, [_I])
+    d("sgemm_b200_version", ctypes.c_char_p, [])
+    d("sgemm", None, _GEMM_ARGS)
+    d("sgemm_basic", None, _GEMM_ARGS)
+
+
+def lib() -> ctypes.CDLL:
+    """Load the shared library once; raise if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(
+                f"{LIB_PATH} is missing: build it with `make -C sgemm.cu_b200` "
+                "(or __graft_entry__.build()); there is no fallback path")
+        l = ctypes.CDLL(LIB_PATH)
+        _declare(l)
+        _lib = l
+    return _lib
+
+
+def status_string(status: int) -> str:
+    return lib().sgemm_b200_status_string(status).decode()
+
+
+def _check(status: int, what: str) -> None:
+    if status != OK:
+        raise SgemmError(status, what)
+
+
+def _f(x: float):
+    return ctypes.byref(ctypes.c_float(x))
+
+
+def _stream_ptr(stream) -> Optional[int]:
+    if stream is None:
+        return None
+    if isinstance(stream, int):
+        return stream
+    return stream.cuda_stream  # torch.cuda.Stream
+
+
+def _mat(t, name: str):
+    """(device pointer, row stride) of a 2-D row-major float32 CUDA tensor."""
+    import torch
+
+    if t.dtype != torch.float32 or t.dim() != 2 or not t.is_cuda:
+        raise ValueError(f"{name} must be a 2-D float32 CUDA tensor")
+    if t.stride(1) != 1:
+        raise ValueError(f"{name} must be row-major with unit column stride")
+    ld = t.stride(0) if t.size(0) > 1 else max(t.size(1), 1)
+    return t.data_ptr(), ld
+
+
+def sgemm(A, B, C, alpha: float = 1.0, beta: float = 0.0, stream=None, config: int = -1) -> None:
+    """C := alpha*A@B + beta*C on the plain FFMA path (in place on C)."""
+    m, k = A.shape
+    k2, n = B.shape
+    if k2 != k or tuple(C.shape) != (m, n):
+        raise ValueError("shape mismatch")
+    pa, lda = _mat(A, "A")
+    pb, ldb = _mat(B, "B")
+    pc, ldc = _mat(C, "C")
+    _check(lib().sgemm_b200_with_config(config, m, n, k, _f(alpha), pa, lda, pb, ldb, _f(beta),
+                                        pc, ldc, _stream_ptr(stream)), "sgemm_b200")
+
+
+def sgemm_basic(A, B, C, alpha: float = 1.0, beta: float = 0.0, stream=None) -> None:
+    """The naive kernel (reference sgemm_basic semantics: always reads C)."""
+    m, k = A.shape
+    n = B.shape[1]
+    pa, lda = _mat(A, "A")
+    pb, ldb = _mat(B, "B")
+    pc, ldc = _mat(C, "C")
+    _check(lib().sgemm_b200_basic(m, n, k, _f(alpha), pa, lda, pb, ldb, _f(beta), pc, ldc,
+                                  _stream_ptr(stream)), "sgemm_b200_basic")
+
+
+def split_workspace_size(path: int, m: int, n: int, k: int) -> int:
+    return int(lib().sgemm_b200_split_workspace_size(path, m, n, k))
+
+
+def sgemm_split(path, A, B, C, alpha: float = 1.0, beta: float = 0.0, workspace=None,
+                stream=None) -> None:
+    """Split-precision tensor-core GEMM; path is 'bf16x6', 'tf32x3' or the enum."""
+    p = PATHS[path] if isinstance(path, str) else int(path)
+    m, k = A.shape
+    n = B.shape[1]
+    pa, lda = _mat(A, "A")
+    pb, ldb = _mat(B, "B")
+    pc, ldc = _mat(C, "C")
+    ws, wsb = (None, 0)
+    if workspace is not None:
+        ws, wsb = workspace.data_ptr(), workspace.numel() * workspace.element_size()
+    _check(lib().sgemm_b200_split(p, m, n, k, _f(alpha), pa, lda, pb, ldb, _f(beta), pc, ldc,
+                                  ws, wsb, _stream_ptr(stream)), "sgemm_b200_split")
+
+
+def gemm(path, A, B, C, alpha: float = 1.0, beta: float = 0.0, stream=None) -> None:
+    p = PATHS[path] if isinstance(path, str) else int(path)
+    m, k = A.shape
+    n = B.shape[1]
+    pa, lda = _mat(A, "A")
+    pb, ldb = _mat(B, "B")
+    pc, ldc = _mat(C, "C")
+    _check(lib().sgemm_b200_gemm(p, m, n, k, _f(alpha), pa, lda, pb, ldb, _f(beta), pc, ldc,
+                                 _stream_ptr(stream)), "sgemm_b200_gemm")
+
+
+def fill_random(X, seed: int, tag: int, dist: int = DIST_UNIFORM_PM1, stream=None) -> None:
+    """Fill a 2-D float32 CUDA tensor from the seeded counter-based generator."""
+    px, ld = _mat(X, "X")
+    _check(lib().sgemm_b200_fill_random(px, X.shape[0], X.shape[1], ld, seed, tag, dist,
+                                        _stream_ptr(stream)), "sgemm_b200_fill_random")
+
+
+def config_names() -> list:
+    l = lib()
+    return [l.sgemm_b200_config_name(i).decode() for i in range(l.sgemm_b200_config_count())]
+
+
+def select_config(m: int, n: int, k: int, A=None, lda: int = 0, B=None, ldb: int = 0) -> int:
+    pa = A.data_ptr() if A is not None else 16
+    pb = B.data_ptr() if B is not None else 16
+    return lib().sgemm_b200_select_config(m, n, k, pa, lda or k, pb, ldb or n, None, n)
+
+
+def device_status() -> int:
+    return lib().sgemm_b200_device_status()
+
+
+def make_problems(specs: Sequence) -> "ctypes.Array":
+    """specs: sequence of (A, B, C, alpha, beta) torch tensors/floats."""
+    arr = (Problem * len(specs))()
+    for i, (A, B, C, alpha, beta) in enumerate(specs):
+        pa, lda = _mat(A, "A")
+        pb, ldb = _mat(B, "B")
+        pc, ldc = _mat(C, "C")
+        arr[i] = Problem(A.shape[0], B.shape[1], A.shape[1], lda, ldb, ldc, alpha, beta, pa, pb,
+                         pc)
+    return arr
+
+
+class GroupedPlan:
+    """Persistent grouped GEMM over a fixed list of problems."""
+
+    def __init__(self, specs: Sequence, tuning_json: Optional[str] = None):
+        self._problems = make_problems(specs)
+        self._keep = specs  # keep tensors alive
+        h = ctypes.c_void_p()
+        _check(lib().sgemm_b200_grouped_plan_create(
+            ctypes.byref(h), self._problems, len(specs),
+            tuning_json.encode() if tuning_json else None), "grouped_plan_create")
+        self._h = h
+
+    def launch(self, stream=None, use_graph: bool = True) -> None:
+        _check(lib().sgemm_b200_grouped_plan_launch(self._h, _stream_ptr(stream),
+                                                    1 if use_graph else 0), "grouped_plan_launch")
+
+    def info(self):
+        t, w, g = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        _check(lib().sgemm_b200_grouped_plan_info(self._h, ctypes.byref(t), ctypes.byref(w),
+                                                  ctypes.byref(g)), "grouped_plan_info")
+        return {"tiles": t.value, "work_items": w.value, "grid_ctas": g.value}
+
+    def close(self) -> None:
+        if self._h:
+            lib().sgemm_b200_grouped_plan_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
