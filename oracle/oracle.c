@@ -7,17 +7,19 @@
  * Contents
  *  - oracle_fill: seeded counter-based generator (restates the generator the
  *    library's fill kernel uses; see rng_* below).
- *  - oracle_sgemm_basic: restatement of kernel_basic
- *    (reference src/kernels/basic.cuh:14-25):
- *        acc = 0; for p in 0..k-1: acc = fma(A[y,p], B[p,x], acc)   (:18-20)
- *        acc *= alpha                                                (:21)
- *        acc = fma(C[y,x], beta, acc)                                (:22-24)
- *    nvcc contracts `acc += a*b` and `acc += c*beta` into single-rounding
- *    FMAs (its default --fmad=true); fmaf() reproduces that rounding here.
- *    With read_c_if_beta_zero == 0 the beta == 0 case skips C entirely, which
- *    is what the reference's tiled kernels do (128x256x8.cuh:365-380).
- *    The per-element summation order is kept (i-p-j loop, j vectorised), so
- *    results are bit-identical to the naive order.
+ *  - oracle_sgemm_basic: the reference's per-element arithmetic, in two
+ *    epilogue flavours (the accumulation is the same for both):
+ *        acc = 0; for p in 0..k-1: acc = fma(A[y,p], B[p,x], acc)
+ *    (kernel_basic, src/kernels/basic.cuh:18-20; the tiled kernels'
+ *    increasing-k chain, src/kernels/128x256x8.cuh:224-239), then
+ *      basic == 0, the tiled kernels (128x256x8.cuh:331-337, :365-380):
+ *        v = acc * alpha;  C = beta != 0 ? fma(C, beta, v) : v   (C unread)
+ *      basic == 1, kernel_basic (basic.cuh:21-24), as nvcc contracts
+ *        `acc *= alpha; acc += c * beta` (default --fmad=true):
+ *        C = fma(acc, alpha, C * beta)                          (C always read)
+ *    Both flavours are pinned bit-for-bit to the reference's own outputs
+ *    (tests/golden/).  The per-element summation order is kept (i-p-j loop,
+ *    j vectorised), so results equal the naive order's bit for bit.
  *  - oracle_dgemm / oracle_dgemm_rows: FP64 C64 = alpha*A*B + beta*C0 with
  *    exact products (24-bit x 24-bit fits in 53 bits) and FP64 sums, plus the
  *    magnitude |alpha|*(|A||B|) + |beta|*|C0| used by the componentwise error.
@@ -117,21 +119,27 @@ int oracle_fill_rows(float* out, const int* row_ids, int nrows, int cols, uint64
     for (int i = 0; i < ib; ++i) {                                                   \
         float* crow = c_rows[i] + j0;                                                \
         for (int j = 0; j < jb; ++j) {                                               \
-            float v = acc[i][j] * alpha;                                             \
-            if (beta != 0.0f || read_c_if_beta_zero) v = fmaf(crow[j], beta, v);     \
+            float v;                                                                 \
+            if (basic) {                                                             \
+                const float cb = crow[j] * beta;                                     \
+                v = fmaf(acc[i][j], alpha, cb);                                      \
+            } else {                                                                 \
+                v = acc[i][j] * alpha;                                               \
+                if (beta != 0.0f) v = fmaf(crow[j], beta, v);                        \
+            }                                                                        \
             crow[j] = v;                                                             \
         }                                                                            \
     }
 
 FMA_TARGET static void block_fma(int ib, int jb, int j0, int k, float alpha,
                                  const float* const* a_rows, const float* B, int ldb, float beta,
-                                 float* const* c_rows, int read_c_if_beta_zero) {
+                                 float* const* c_rows, int basic) {
     BLOCK_BODY
 }
 
 static void block_plain(int ib, int jb, int j0, int k, float alpha, const float* const* a_rows,
                         const float* B, int ldb, float beta, float* const* c_rows,
-                        int read_c_if_beta_zero) {
+                        int basic) {
     BLOCK_BODY
 }
 
@@ -163,7 +171,7 @@ int oracle_max_threads(void) {
  * the general form behind both entry points below. */
 static int sgemm_rows_impl(int nrows, const int* row_ids, int n, int k, float alpha,
                            const float* A, int lda, const float* B, int ldb, float beta,
-                           float* C, int ldc, int c_is_compact, int read_c_if_beta_zero,
+                           float* C, int ldc, int c_is_compact, int basic,
                            int nthreads) {
     if (nrows < 0 || n < 0 || k < 0) return 1;
     set_threads(nthreads);
@@ -183,29 +191,29 @@ static int sgemm_rows_impl(int nrows, const int* row_ids, int n, int k, float al
         for (int j0 = 0; j0 < n; j0 += JB) {
             const int jb = n - j0 < JB ? n - j0 : JB;
             if (fma_ok)
-                block_fma(ib, jb, j0, k, alpha, a_rows, B, ldb, beta, c_rows, read_c_if_beta_zero);
+                block_fma(ib, jb, j0, k, alpha, a_rows, B, ldb, beta, c_rows, basic);
             else
                 block_plain(ib, jb, j0, k, alpha, a_rows, B, ldb, beta, c_rows,
-                            read_c_if_beta_zero);
+                            basic);
         }
     }
     return 0;
 }
 
 int oracle_sgemm_basic(int m, int n, int k, float alpha, const float* A, int lda, const float* B,
-                       int ldb, float beta, float* C, int ldc, int read_c_if_beta_zero,
+                       int ldb, float beta, float* C, int ldc, int basic,
                        int nthreads) {
     return sgemm_rows_impl(m, NULL, n, k, alpha, A, lda, B, ldb, beta, C, ldc, 0,
-                           read_c_if_beta_zero, nthreads);
+                           basic, nthreads);
 }
 
 /* Rows row_ids[0..nrows) of the product; A is the full matrix, C is compact
  * (nrows x n, row stride ldc) and holds the beta-input rows on entry. */
 int oracle_sgemm_basic_rows(int nrows, const int* row_ids, int n, int k, float alpha,
                             const float* A, int lda, const float* B, int ldb, float beta,
-                            float* C, int ldc, int read_c_if_beta_zero, int nthreads) {
+                            float* C, int ldc, int basic, int nthreads) {
     return sgemm_rows_impl(nrows, row_ids, n, k, alpha, A, lda, B, ldb, beta, C, ldc, 1,
-                           read_c_if_beta_zero, nthreads);
+                           basic, nthreads);
 }
 
 /* ------------------------------------------------------------ FP64 GEMM -- */

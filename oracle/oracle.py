@@ -73,27 +73,30 @@ def fill_rows(row_ids, cols: int, seed: int, tag: int, dist: int) -> np.ndarray:
 
 
 def sgemm_basic(A: np.ndarray, B: np.ndarray, C: np.ndarray, alpha: float, beta: float,
-                read_c_if_beta_zero: bool = True, threads: int = 0) -> np.ndarray:
-    """Restatement of kernel_basic; returns a new array (C is not modified)."""
+                basic: bool = True, threads: int = 0) -> np.ndarray:
+    """The reference's per-element arithmetic; returns a new array (C is not
+    modified).  basic=True: kernel_basic's epilogue fma(acc, alpha, c*beta),
+    C always read.  basic=False: the tiled kernels' fma(c, beta, acc*alpha),
+    C not read when beta == 0."""
     m, k = A.shape
     n = B.shape[1]
     out = np.ascontiguousarray(C, dtype=np.float32).copy()
     A = np.ascontiguousarray(A, dtype=np.float32)
     B = np.ascontiguousarray(B, dtype=np.float32)
     cpu().oracle_sgemm_basic(m, n, k, alpha, A, max(k, 1), B, max(n, 1), beta, out, max(n, 1),
-                             1 if read_c_if_beta_zero else 0, threads)
+                             1 if basic else 0, threads)
     return out
 
 
 def sgemm_basic_rows(row_ids, A: np.ndarray, B: np.ndarray, C_rows: np.ndarray, alpha: float,
-                     beta: float, read_c_if_beta_zero: bool = True, threads: int = 0) -> np.ndarray:
+                     beta: float, basic: bool = True, threads: int = 0) -> np.ndarray:
     ids = np.ascontiguousarray(row_ids, dtype=np.int32)
     m, k = A.shape
     n = B.shape[1]
     out = np.ascontiguousarray(C_rows, dtype=np.float32).copy()
     cpu().oracle_sgemm_basic_rows(len(ids), ids, n, k, alpha, np.ascontiguousarray(A), k,
                                   np.ascontiguousarray(B), n, beta, out, n,
-                                  1 if read_c_if_beta_zero else 0, threads)
+                                  1 if basic else 0, threads)
     return out
 
 

@@ -3,8 +3,10 @@
 //
 // sgemm_b200_basic replaces sgemm_basic()/kernel_basic
 // (src/sgemm.cuh:92-113, src/kernels/basic.cuh:1-26): sequential accumulation
-// acc = fma(A[y,p], B[p,x], acc) for p = 0..k-1, then acc *= alpha and
-// acc = fma(C, beta, acc).  Like the reference it always reads C.
+// acc = fma(A[y,p], B[p,x], acc) for p = 0..k-1, then the epilogue
+// `acc *= alpha; acc += c * beta` evaluated the way nvcc contracts it in the
+// reference (basic.cuh:21-24): C = fma(acc, alpha, c * beta).  Outputs equal
+// the reference kernel's bit for bit.  Like the reference it always reads C.
 #include "common.h"
 #include "rng.h"
 
@@ -17,9 +19,8 @@ __global__ void basic_kernel(int m, int n, int k, float alpha, const float* __re
     if (x >= n || y >= m) return;
     float acc = 0.0f;
     for (int p = 0; p < k; ++p) acc = fmaf(A[(int64_t)y * lda + p], B[(int64_t)p * ldb + x], acc);
-    acc = __fmul_rn(acc, alpha);
     const float c = C[(int64_t)y * ldc + x];
-    C[(int64_t)y * ldc + x] = fmaf(c, beta, acc);
+    C[(int64_t)y * ldc + x] = fmaf(acc, alpha, __fmul_rn(c, beta));
 }
 
 __global__ void fill_kernel(float* X, int rows, int cols, int ld, uint64_t seed, uint32_t tag,

@@ -91,6 +91,22 @@ bool encode_tensor_map_2d(CUtensorMap* map, CUtensorMapDataType dtype, const voi
     return r == CUDA_SUCCESS;
 }
 
+bool encode_tensor_map_3d(CUtensorMap* map, CUtensorMapDataType dtype, const void* base,
+                          uint64_t inner, uint64_t mid, uint64_t outer, uint64_t mid_stride_bytes,
+                          uint64_t outer_stride_bytes, uint32_t box_inner, uint32_t box_mid,
+                          uint32_t box_outer, CUtensorMapSwizzle swizzle) {
+    auto fn = get_encode_fn();
+    if (!fn) return false;
+    cuuint64_t dims[3] = {inner, mid, outer};
+    cuuint64_t strides[2] = {mid_stride_bytes, outer_stride_bytes};
+    cuuint32_t box[3] = {box_inner, box_mid, box_outer};
+    cuuint32_t estr[3] = {1, 1, 1};
+    CUresult r = fn(map, dtype, 3, const_cast<void*>(base), dims, strides, box, estr,
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, swizzle, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
+
 int check_gemm_args(int m, int n, int k, const float* alpha, const void* A, int lda,
                     const void* B, int ldb, const float* beta, const void* C, int ldc) {
     if (m < 0 || n < 0 || k < 0) return SGEMM_B200_ERR_INVALID_ARG;

@@ -45,6 +45,12 @@ bool encode_tensor_map_2d(CUtensorMap* map, CUtensorMapDataType dtype, const voi
                           uint64_t inner_elems, uint64_t outer_elems, uint64_t row_stride_bytes,
                           uint32_t box_inner, uint32_t box_outer, CUtensorMapSwizzle swizzle);
 
+// 3-D variant: dims {inner, mid, outer}, byte strides of mid and outer.
+bool encode_tensor_map_3d(CUtensorMap* map, CUtensorMapDataType dtype, const void* base,
+                          uint64_t inner, uint64_t mid, uint64_t outer, uint64_t mid_stride_bytes,
+                          uint64_t outer_stride_bytes, uint32_t box_inner, uint32_t box_mid,
+                          uint32_t box_outer, CUtensorMapSwizzle swizzle);
+
 // Shape checks common to every entry point.  Returns SGEMM_B200_OK or
 // SGEMM_B200_ERR_INVALID_ARG.
 int check_gemm_args(int m, int n, int k, const float* alpha, const void* A, int lda,

@@ -84,8 +84,9 @@ int plain_config_tile(int cfg, int* bm, int* bn) {
 }
 
 // Pick the configuration with the smallest modelled time:
-//   waves(cfg) * tile_work(cfg) / efficiency(cfg)
-// where waves = ceil(tiles / (SMs * resident CTAs per SM)).
+//   waves(cfg) * tile_work(cfg) * resident(cfg) / efficiency(cfg)
+// where waves = ceil(tiles / (SMs * resident CTAs per SM)): the resident
+// CTAs of one wave share an SM, so each takes `resident` times as long.
 int plain_select(int m, int n, int k, const float* A, int lda, const float* B, int ldb) {
     using namespace ffma;
     const int base = (k == 0 || tma_ok(A, lda, B, ldb)) ? 0 : kNumPerLoader;
@@ -98,8 +99,7 @@ int plain_select(int m, int n, int k, const float* A, int lda, const float* B, i
         const double tiles = double(div_up(m, cd.bm)) * div_up(n, cd.bn);
         const double slots = double(sms) * occupancy(c);
         const double waves = std::ceil(tiles / slots);
-        // Work per tile, with its resident-CTA share of the SM.
-        const double t = waves * double(cd.bm) * cd.bn / (cd.efficiency * occupancy(c));
+        const double t = waves * double(cd.bm) * cd.bn * occupancy(c) / cd.efficiency;
         if (t < best_t * 0.999) {
             best_t = t;
             best = c;

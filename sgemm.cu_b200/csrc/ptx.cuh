@@ -98,6 +98,16 @@ __device__ __forceinline__ void tma_load_2d(void* smem_dst, const void* tmap, ui
         : "memory");
 }
 
+// 3-D tiled tensor load (c0 innermost).
+__device__ __forceinline__ void tma_load_3d(void* smem_dst, const void* tmap, uint64_t* bar,
+                                            int32_t c0, int32_t c1, int32_t c2) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%3, %4, %5}], [%2];" ::"r"(smem_u32(smem_dst)),
+        "l"(reinterpret_cast<uint64_t>(tmap)), "r"(smem_u32(bar)), "r"(c0), "r"(c1), "r"(c2)
+        : "memory");
+}
+
 // ----------------------------------------------------------------- cp.async --
 
 // 4-byte async copy; when `valid` is false the destination is zero-filled and
@@ -211,6 +221,21 @@ __device__ __forceinline__ uint64_t sw128_kmajor_desc(uint32_t smem_addr) {
     d |= static_cast<uint64_t>(1024u >> 4) << 32;
     d |= static_cast<uint64_t>(1u) << 46;
     d |= static_cast<uint64_t>(2u) << 61;
+    return d;
+}
+
+// Same for the 64-byte swizzle (rows of 64 bytes, 8-row atoms of 512 bytes),
+// layout type 4, stride byte offset 512 B.  Advancing the start address by
+// 32 bytes selects the second 32-byte K slice of every row; the tile base
+// must be 512-byte aligned so the hardware's address-based XOR matches the
+// pattern TMA wrote.
+__device__ __forceinline__ uint64_t sw64_kmajor_desc(uint32_t smem_addr) {
+    uint64_t d = 0;
+    d |= static_cast<uint64_t>((smem_addr >> 4) & 0x3FFFu);
+    d |= static_cast<uint64_t>(1u) << 16;
+    d |= static_cast<uint64_t>(512u >> 4) << 32;
+    d |= static_cast<uint64_t>(1u) << 46;
+    d |= static_cast<uint64_t>(4u) << 61;
     return d;
 }
 

@@ -1,8 +1,486 @@
-// split.cu — split-precision tensor-core path (under construction).
+// split.cu — split-precision FP32 GEMM on the 5th-generation tensor cores.
+//
+// No reference counterpart: the reference has no tensor-core path at all
+// (src/kernels/*.cuh are FFMA only).  The contract is the reference sgemm()'s
+// (src/sgemm.cuh:19-30): C := alpha*A*B + beta*C, FP32 row-major, beta == 0
+// never reads C.
+//
+// BF16X6: every FP32 operand x is split exactly into three BF16 terms
+//   x_h = bf16(x), x_m = bf16(x - x_h), x_l = bf16(x - x_h - x_m)
+// and A*B is formed from the six cross products that carry the FP32 bits:
+//   hh + (hm + mh + hl + lh + mm)       (ml, lm, ll are below 2^-24 |a||b|).
+// TF32X3: x_h = tf32(x), x_l = tf32(x - x_h);  A*B = hh + (hl + lh).
+//
+// The products run as tcgen05.mma (kind::f16 with BF16 inputs, or
+// kind::tf32) with FP32 accumulation in tensor memory.  The dominant hh term
+// and the small correction terms accumulate in two separate TMEM accumulators
+// (D1, D2) that the epilogue adds once, so the correction sum's rounding is
+// ~2^-8 smaller than the main sum's.
+//
+// Kernel shape: one CTA of 4 warps per 128 x 256 output tile.
+//   warp 0 / lane 0  TMA producer: one 3-D box per operand per stage brings
+//                    all split planes of a K slice (64-byte rows, 64-byte swizzle)
+//   warp 1 / lane 0  MMA issuer: tcgen05.mma M=128 N=256, commit per stage
+//   warps 0..3       epilogue: tcgen05.ld 32 lanes x 32 columns, alpha/beta,
+//                    float4 stores (warp w owns TMEM lanes / rows 32w..32w+31)
+// Every mbarrier wait is bounded (ptx.cuh); on expiry the status word is set,
+// in-flight copies and MMAs are drained with bounded waits, TMEM is freed.
+//
+// A split pre-pass writes the operand planes (A as [split][M][Kp], B
+// transposed to [split][N][Kp], both K-major) into a workspace.
+#include <cuda_bf16.h>
+
+#include <cstring>
+
 #include "common.h"
+#include "plain.h"
+#include "ptx.cuh"
+
+namespace sgb {
+namespace split {
+
+constexpr int BM = 128, BN = 256, THREADS = 128;
+constexpr int TMEM_COLS = 512;  // D1 at column 0, D2 at column BN
+
+template <int PATH>
+struct Traits;
+
+template <>
+struct Traits<SGEMM_B200_PATH_BF16X6> {
+    static constexpr int NSPLIT = 3, ESZ = 2, BK = 32, KMMA = 16, STAGES = 3;
+    static constexpr uint32_t FMT = 1;  // BF16
+    static constexpr int NPROD = 6;
+    // (a split, b split, accumulator) in issue order
+    __device__ static constexpr int pa(int i) { return i == 0 ? 0 : (i == 1 || i == 3) ? 0 : (i == 5 ? 1 : (i == 2 ? 1 : 2)); }
+    __device__ static constexpr int pb(int i) { return i == 0 ? 0 : i == 1 ? 1 : i == 2 ? 0 : i == 3 ? 2 : i == 4 ? 0 : 1; }
+};
+
+template <>
+struct Traits<SGEMM_B200_PATH_TF32X3> {
+    static constexpr int NSPLIT = 2, ESZ = 4, BK = 16, KMMA = 8, STAGES = 4;
+    static constexpr uint32_t FMT = 2;  // TF32
+    static constexpr int NPROD = 3;
+    __device__ static constexpr int pa(int i) { return i == 2 ? 1 : 0; }
+    __device__ static constexpr int pb(int i) { return i == 1 ? 1 : 0; }
+};
+
+template <int PATH>
+struct Layout {
+    using T = Traits<PATH>;
+    static constexpr int ROW_BYTES = T::BK * T::ESZ;  // 64: one swizzle-64 row
+    static_assert(ROW_BYTES == 64, "64-byte K rows");
+    static constexpr int A_PLANE = BM * ROW_BYTES;    // 8 KB
+    static constexpr int B_PLANE = BN * ROW_BYTES;    // 16 KB
+    static constexpr int A_BYTES = T::NSPLIT * A_PLANE;
+    static constexpr int B_BYTES = T::NSPLIT * B_PLANE;
+    static constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
+    static constexpr int SMEM_BYTES = T::STAGES * STAGE_BYTES + 1024;
+    static_assert(SMEM_BYTES <= 227 * 1024, "shared memory budget");
+};
+
+struct Params {
+    int m, n, k;
+    int ldc;
+    float alpha, beta;
+    float* C;
+    int* status;
+    int tiles_m, tiles_n;
+    int vec_c;
+};
+
+__device__ __forceinline__ void tile_coords(int bid, int tiles_m, int tiles_n, int& tm, int& tn) {
+    constexpr int G = 8;
+    const int per_group = G * tiles_n;
+    const int gid = bid / per_group;
+    const int first = gid * G;
+    const int gsz = min(tiles_m - first, G);
+    const int r = bid % per_group;
+    tm = first + r % gsz;
+    tn = r / gsz;
+}
+
+template <int PATH>
+__global__ void __launch_bounds__(THREADS, 1)
+    split_gemm_kernel(const __grid_constant__ CUtensorMap tmA,
+                      const __grid_constant__ CUtensorMap tmB, const Params p) {
+    using T = Traits<PATH>;
+    using L = Layout<PATH>;
+    extern __shared__ uint8_t smem_raw[];
+    __shared__ __align__(8) uint64_t full_bar[T::STAGES];
+    __shared__ __align__(8) uint64_t empty_bar[T::STAGES];
+    __shared__ __align__(8) uint64_t done_bar;
+    __shared__ uint32_t tmem_base_s;
+    __shared__ volatile int abort_s;
+    __shared__ int consumed_s;
+    uint8_t* smem = reinterpret_cast<uint8_t*>(
+        (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
+
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    int tm, tn;
+    tile_coords(blockIdx.x, p.tiles_m, p.tiles_n, tm, tn);
+    const int m0 = tm * BM, n0 = tn * BN;
+    const int nk = (p.k + T::BK - 1) / T::BK;
+
+    if (tid == 0) {
+        for (int s = 0; s < T::STAGES; ++s) {
+            mbar_init(&full_bar[s], 1);
+            mbar_init(&empty_bar[s], 1);
+        }
+        mbar_init(&done_bar, 1);
+        abort_s = 0;
+        consumed_s = 0;
+        fence_barrier_init();
+        tma_prefetch_desc(&tmA);
+        tma_prefetch_desc(&tmB);
+    }
+    if (warp == 0) {
+        tmem_alloc(&tmem_base_s, TMEM_COLS);
+        tmem_relinquish();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = tmem_base_s;
+
+    int issued = 0;
+    if (warp == 0 && lane == 0) {
+        // ---------------------------------------------------- TMA producer --
+        for (int kb = 0; kb < nk; ++kb) {
+            const int s = kb % T::STAGES;
+            if (kb >= T::STAGES) {
+                if (!mbar_wait(&empty_bar[s], ((kb / T::STAGES) - 1) & 1) || abort_s) {
+                    abort_s = 1;
+                    atomicExch(p.status, SGEMM_B200_ERR_TIMEOUT);
+                    break;
+                }
+            }
+            uint8_t* st = smem + s * L::STAGE_BYTES;
+            mbar_arrive_expect_tx(&full_bar[s], L::STAGE_BYTES);
+            tma_load_3d(st, &tmA, &full_bar[s], kb * T::BK, m0, 0);
+            tma_load_3d(st + L::A_BYTES, &tmB, &full_bar[s], kb * T::BK, n0, 0);
+            ++issued;
+        }
+    } else if (warp == 1 && lane == 0) {
+        // ------------------------------------------------------ MMA issuer --
+        constexpr uint32_t idesc = make_idesc(T::FMT, BM, BN);
+        int kb = 0;
+        for (; kb < nk; ++kb) {
+            const int s = kb % T::STAGES;
+            if (!mbar_wait(&full_bar[s], (kb / T::STAGES) & 1) || abort_s) {
+                abort_s = 1;
+                atomicExch(p.status, SGEMM_B200_ERR_TIMEOUT);
+                break;
+            }
+            tc_fence_after();
+            const uint32_t a0 = smem_u32(smem + s * L::STAGE_BYTES);
+            const uint32_t b0 = a0 + L::A_BYTES;
+#pragma unroll
+            for (int j = 0; j < T::BK / T::KMMA; ++j) {
+                const uint32_t koff = j * T::KMMA * T::ESZ;  // 32 bytes per MMA K slice
+#pragma unroll
+                for (int i = 0; i < T::NPROD; ++i) {
+                    const uint64_t ad = sw64_kmajor_desc(a0 + T::pa(i) * L::A_PLANE + koff);
+                    const uint64_t bd = sw64_kmajor_desc(b0 + T::pb(i) * L::B_PLANE + koff);
+                    const uint32_t d = tmem + (i == 0 ? 0u : static_cast<uint32_t>(BN));
+                    // first product into each accumulator overwrites it
+                    const uint32_t acc = (kb > 0 || j > 0 || (i > 1)) ? 1u : 0u;
+                    if constexpr (T::FMT == 1)
+                        mma_bf16_ss(d, ad, bd, idesc, acc);
+                    else
+                        mma_tf32_ss(d, ad, bd, idesc, acc);
+                }
+            }
+            mma_commit(&empty_bar[s]);  // frees the stage once these MMAs read it
+        }
+        consumed_s = kb;
+        mma_commit(&done_bar);  // arrives when every MMA issued above has completed
+    }
+
+    // ------------------------------------------------------------ epilogue --
+    __syncwarp();
+    bool ok = nk == 0 ? true : mbar_wait(&done_bar, 0);
+    if (!ok) atomicExch(p.status, SGEMM_B200_ERR_TIMEOUT);
+    ok = ok && !abort_s;
+    tc_fence_after();
+
+    const int row = m0 + warp * 32 + lane;
+    const uint32_t trow = tmem + (static_cast<uint32_t>(warp * 32) << 16);
+    if (ok) {
+        for (int c = 0; c < BN / 32; ++c) {
+            const int col0 = n0 + c * 32;
+            if (col0 >= p.n) break;  // uniform across the warp
+            uint32_t d1[32], d2[32];
+            if (nk > 0) {
+                tmem_ld_32x32b_x32(trow + c * 32, d1);
+                tmem_ld_32x32b_x32(trow + BN + c * 32, d2);
+                tmem_ld_wait();
+            } else {
+#pragma unroll
+                for (int j = 0; j < 32; ++j) d1[j] = d2[j] = 0u;
+            }
+            if (row < p.m) {
+                float* crow = p.C + (int64_t)row * p.ldc + col0;
+                float v[32];
+#pragma unroll
+                for (int j = 0; j < 32; ++j)
+                    v[j] = __fmul_rn(__fadd_rn(__uint_as_float(d1[j]), __uint_as_float(d2[j])),
+                                     p.alpha);
+                if (p.vec_c && col0 + 31 < p.n) {
+#pragma unroll
+                    for (int q = 0; q < 8; ++q) {
+                        float4* dst = reinterpret_cast<float4*>(crow + 4 * q);
+                        float4 o = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+                        if (p.beta != 0.0f) {
+                            const float4 old = *dst;
+                            o.x = fmaf(old.x, p.beta, o.x);
+                            o.y = fmaf(old.y, p.beta, o.y);
+                            o.z = fmaf(old.z, p.beta, o.z);
+                            o.w = fmaf(old.w, p.beta, o.w);
+                        }
+                        *dst = o;
+                    }
+                } else {
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) {
+                        if (col0 + j < p.n) {
+                            float o = v[j];
+                            if (p.beta != 0.0f) o = fmaf(crow[j], p.beta, o);
+                            crow[j] = o;
+                        }
+                    }
+                }
+            }
+        }
+    }
+
+    // ------------------------------------------------------------ teardown --
+    tc_fence_before();
+    __syncthreads();  // every TMEM load is done; consumed_s is visible
+    if (warp == 0) {
+        if (lane == 0) {
+            // Copies the MMA issuer never consumed (only after an abort) must
+            // land before this CTA's shared memory is released.
+            for (int j = consumed_s; j < issued; ++j)
+                if (!mbar_wait(&full_bar[j % T::STAGES], (j / T::STAGES) & 1)) break;
+        }
+        __syncwarp();
+        tmem_dealloc(tmem, TMEM_COLS);
+    }
+}
+
+// ------------------------------------------------------------ split pre-pass --
+
+__device__ __forceinline__ float tf32_rna(float x) {
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+    return __uint_as_float(r);
+}
+
+template <int PATH>
+__device__ __forceinline__ void split_value(float x, float (&out)[3]) {
+    if constexpr (PATH == SGEMM_B200_PATH_BF16X6) {
+        const float h = __bfloat162float(__float2bfloat16_rn(x));
+        const float r1 = __fsub_rn(x, h);
+        const float mm = __bfloat162float(__float2bfloat16_rn(r1));
+        const float r2 = __fsub_rn(r1, mm);
+        out[0] = h;
+        out[1] = mm;
+        out[2] = __bfloat162float(__float2bfloat16_rn(r2));
+    } else {
+        const float h = tf32_rna(x);
+        out[0] = h;
+        out[1] = tf32_rna(__fsub_rn(x, h));
+        out[2] = 0.0f;
+    }
+}
+
+// Store 8 consecutive split values (one per plane) as 16-byte vectors.
+template <int PATH>
+__device__ __forceinline__ void store8(uint8_t* plane0, int64_t plane_bytes, int64_t elem,
+                                       const float (&v)[8][3]) {
+    using T = Traits<PATH>;
+#pragma unroll
+    for (int s = 0; s < T::NSPLIT; ++s) {
+        uint8_t* dst = plane0 + s * plane_bytes + elem * T::ESZ;
+        if constexpr (T::ESZ == 2) {
+            uint32_t w[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const __nv_bfloat162 b2 = __floats2bfloat162_rn(v[2 * q][s], v[2 * q + 1][s]);
+                w[q] = *reinterpret_cast<const uint32_t*>(&b2);
+            }
+            *reinterpret_cast<uint4*>(dst) = make_uint4(w[0], w[1], w[2], w[3]);
+        } else {
+            reinterpret_cast<float4*>(dst)[0] = make_float4(v[0][s], v[1][s], v[2][s], v[3][s]);
+            reinterpret_cast<float4*>(dst)[1] = make_float4(v[4][s], v[5][s], v[6][s], v[7][s]);
+        }
+    }
+}
+
+// A [m x lda] -> planes [split][m][kp], zero in columns k..kp-1.  One thread
+// per 8 consecutive k of one row.
+template <int PATH>
+__global__ void split_a_kernel(const float* __restrict__ A, int m, int k, int lda, int kp,
+                               uint8_t* __restrict__ out) {
+    using T = Traits<PATH>;
+    const int64_t plane_bytes = (int64_t)m * kp * T::ESZ;
+    const int chunks = kp / 8;
+    const int64_t total = (int64_t)m * chunks;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t r = i / chunks;
+        const int c0 = (int)(i % chunks) * 8;
+        float v[8][3];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            const float x = c0 + j < k ? A[r * lda + c0 + j] : 0.0f;
+            split_value<PATH>(x, v[j]);
+        }
+        store8<PATH>(out, plane_bytes, r * kp + c0, v);
+    }
+}
+
+// B [k x ldb] -> transposed planes [split][n][kp] via 64 x 64 shared tiles.
+template <int PATH>
+__global__ void split_bt_kernel(const float* __restrict__ B, int k, int n, int ldb, int kp,
+                                uint8_t* __restrict__ out) {
+    using T = Traits<PATH>;
+    __shared__ float tile[64][65];
+    const int k0 = blockIdx.y * 64, n0 = blockIdx.x * 64;
+    const int tx = threadIdx.x % 64, ty = threadIdx.x / 64;  // 256 threads
+#pragma unroll 4
+    for (int i = 0; i < 16; ++i) {
+        const int kk = i * 4 + ty;
+        const int gk = k0 + kk, gn = n0 + tx;
+        tile[kk][tx] = (gk < k && gn < n) ? B[(int64_t)gk * ldb + gn] : 0.0f;
+    }
+    __syncthreads();
+    const int64_t plane_bytes = (int64_t)n * kp * T::ESZ;
+    // thread -> (row nn of B^T, 8-wide k chunk kc); 64 rows x 8 chunks = 512 items
+    for (int item = threadIdx.x; item < 512; item += 256) {
+        const int nn = item / 8, kc = (item % 8) * 8;
+        const int gn = n0 + nn, gk = k0 + kc;
+        if (gn >= n || gk >= kp) continue;
+        float v[8][3];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) split_value<PATH>(tile[kc + j][nn], v[j]);
+        store8<PATH>(out, plane_bytes, (int64_t)gn * kp + gk, v);
+    }
+}
+
+template <int PATH>
+static size_t workspace_bytes(int m, int n, int k, size_t* a_bytes_out = nullptr) {
+    using T = Traits<PATH>;
+    const int64_t kp = ((int64_t)k + 7) / 8 * 8;
+    const size_t a = (size_t)T::NSPLIT * m * kp * T::ESZ;
+    const size_t b = (size_t)T::NSPLIT * n * kp * T::ESZ;
+    const size_t a_al = (a + 1023) / 1024 * 1024;
+    if (a_bytes_out) *a_bytes_out = a_al;
+    return a_al + b + 1024;  // + alignment slack for the base
+}
+
+template <int PATH>
+static int launch(int m, int n, int k, float alpha, const float* A, int lda, const float* B,
+                  int ldb, float beta, float* C, int ldc, void* ws, size_t ws_bytes,
+                  cudaStream_t stream) {
+    using T = Traits<PATH>;
+    using L = Layout<PATH>;
+    size_t a_bytes = 0;
+    const size_t need = workspace_bytes<PATH>(m, n, k, &a_bytes);
+    if (ws_bytes < need) return SGEMM_B200_ERR_NO_MEMORY;
+    uint8_t* base = reinterpret_cast<uint8_t*>(
+        (reinterpret_cast<uintptr_t>(ws) + 1023) & ~static_cast<uintptr_t>(1023));
+    uint8_t* wa = base;
+    uint8_t* wb = base + a_bytes;
+    const int kp = (k + 7) / 8 * 8;
+
+    {
+        const int64_t total = (int64_t)m * (kp / 8);
+        int64_t blocks = (total + 255) / 256;
+        if (blocks > 148 * 32) blocks = 148 * 32;
+        split_a_kernel<PATH><<<(int)blocks, 256, 0, stream>>>(A, m, k, lda, kp, wa);
+        dim3 g(div_up(n, 64), div_up(kp, 64));
+        split_bt_kernel<PATH><<<g, 256, 0, stream>>>(B, k, n, ldb, kp, wb);
+    }
+
+    const CUtensorMapDataType dt =
+        T::ESZ == 2 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+    CUtensorMap tmA, tmB;
+    std::memset(&tmA, 0, sizeof(tmA));
+    std::memset(&tmB, 0, sizeof(tmB));
+    const uint64_t row = (uint64_t)kp * T::ESZ;
+    if (!encode_tensor_map_3d(&tmA, dt, wa, (uint64_t)k, (uint64_t)m, T::NSPLIT, row,
+                              row * (uint64_t)m, T::BK, BM, T::NSPLIT,
+                              CU_TENSOR_MAP_SWIZZLE_64B) ||
+        !encode_tensor_map_3d(&tmB, dt, wb, (uint64_t)k, (uint64_t)n, T::NSPLIT, row,
+                              row * (uint64_t)n, T::BK, BN, T::NSPLIT,
+                              CU_TENSOR_MAP_SWIZZLE_64B))
+        return SGEMM_B200_ERR_CUDA;
+
+    Params p;
+    p.m = m;
+    p.n = n;
+    p.k = k;
+    p.ldc = ldc;
+    p.alpha = alpha;
+    p.beta = beta;
+    p.C = C;
+    p.status = device_status_ptr();
+    if (!p.status) return SGEMM_B200_ERR_CUDA;
+    p.tiles_m = div_up(m, BM);
+    p.tiles_n = div_up(n, BN);
+    p.vec_c = (ldc % 4 == 0) && (reinterpret_cast<uintptr_t>(C) % 16 == 0);
+
+    static bool attr_set[64] = {false};
+    const int dev = device_info().device;
+    if (dev >= 0 && dev < 64 && !attr_set[dev]) {
+        cudaFuncSetAttribute(split_gemm_kernel<PATH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             L::SMEM_BYTES);
+        attr_set[dev] = true;
+    }
+    split_gemm_kernel<PATH><<<p.tiles_m * p.tiles_n, THREADS, L::SMEM_BYTES, stream>>>(tmA, tmB,
+                                                                                      p);
+    return cuda_status(cudaGetLastError());
+}
+
+}  // namespace split
+
+int split_launch(int path, int m, int n, int k, float alpha, const float* A, int lda,
+                 const float* B, int ldb, float beta, float* C, int ldc, void* ws,
+                 size_t ws_bytes, cudaStream_t stream) {
+    if (m == 0 || n == 0) return SGEMM_B200_OK;
+    if (!device_is_sm100()) return SGEMM_B200_ERR_UNSUPPORTED;
+    if (k == 0)  // C = beta*C: no products to split
+        return plain_launch(-1, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, stream);
+    const size_t need = path == SGEMM_B200_PATH_BF16X6
+                            ? split::workspace_bytes<SGEMM_B200_PATH_BF16X6>(m, n, k)
+                            : split::workspace_bytes<SGEMM_B200_PATH_TF32X3>(m, n, k);
+    bool owned = false;
+    if (!ws) {
+        cudaError_t e = cudaMallocAsync(&ws, need, stream);
+        if (e != cudaSuccess) return cuda_status(e);
+        ws_bytes = need;
+        owned = true;
+    }
+    int s;
+    if (path == SGEMM_B200_PATH_BF16X6)
+        s = split::launch<SGEMM_B200_PATH_BF16X6>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, ws,
+                                                  ws_bytes, stream);
+    else
+        s = split::launch<SGEMM_B200_PATH_TF32X3>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, ws,
+                                                  ws_bytes, stream);
+    if (owned) cudaFreeAsync(ws, stream);
+    return s;
+}
+
+}  // namespace sgb
 
 extern "C" size_t sgemm_b200_split_workspace_size(int path, int m, int n, int k) {
-    (void)path; (void)m; (void)n; (void)k;
+    if (m <= 0 || n <= 0 || k <= 0) return 0;
+    if (path == SGEMM_B200_PATH_BF16X6)
+        return sgb::split::workspace_bytes<SGEMM_B200_PATH_BF16X6>(m, n, k);
+    if (path == SGEMM_B200_PATH_TF32X3)
+        return sgb::split::workspace_bytes<SGEMM_B200_PATH_TF32X3>(m, n, k);
     return 0;
 }
 
@@ -10,10 +488,14 @@ extern "C" int sgemm_b200_split(int path, int m, int n, int k, const float* alph
                                 int lda, const float* B, int ldb, const float* beta, float* C,
                                 int ldc, void* workspace, size_t workspace_bytes,
                                 sgemm_b200_stream_t stream) {
-    (void)path; (void)m; (void)n; (void)k; (void)alpha; (void)A; (void)lda; (void)B; (void)ldb;
-    (void)beta; (void)C; (void)ldc; (void)workspace; (void)workspace_bytes; (void)stream;
-    sgb::set_last_status(SGEMM_B200_ERR_UNSUPPORTED);
-    return SGEMM_B200_ERR_UNSUPPORTED;
+    int s = sgb::check_gemm_args(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+    if (s == SGEMM_B200_OK && path != SGEMM_B200_PATH_BF16X6 && path != SGEMM_B200_PATH_TF32X3)
+        s = SGEMM_B200_ERR_INVALID_ARG;
+    if (s == SGEMM_B200_OK)
+        s = sgb::split_launch(path, m, n, k, *alpha, A, lda, B, ldb, *beta, C, ldc, workspace,
+                              workspace_bytes, sgb::as_stream(stream));
+    sgb::set_last_status(s);
+    return s;
 }
 
 extern "C" int sgemm_b200_gemm(int path, int m, int n, int k, const float* alpha, const float* A,
@@ -21,5 +503,6 @@ extern "C" int sgemm_b200_gemm(int path, int m, int n, int k, const float* alpha
                                int ldc, sgemm_b200_stream_t stream) {
     if (path == SGEMM_B200_PATH_PLAIN)
         return sgemm_b200(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, stream);
-    return sgemm_b200_split(path, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, nullptr, 0, stream);
+    return sgemm_b200_split(path, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, nullptr, 0,
+                            stream);
 }

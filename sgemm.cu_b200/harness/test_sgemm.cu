@@ -5,9 +5,11 @@
 // the chosen path, one call of the naive kernel (sgemm_b200_basic, the
 // reference's sgemm_basic), then the reference's comparison (relative error
 // <= 1e-4, NaN/Inf are failures).  Differences from the reference harness:
-// reproducible seeded inputs instead of srand(time(NULL)); the plain path is
-// also checked for bit-exact equality; the exit status is non-zero when any
-// size fails (the reference always exits 0, test.cu:120).
+// reproducible seeded inputs instead of srand(time(NULL)); the count of
+// bit-identical elements is reported (the naive kernel's epilogue rounds
+// fma(acc, alpha, c*beta), the tiled path's fma(c, beta, acc*alpha), so a
+// last-bit difference is expected where beta != 0); the exit status is
+// non-zero when any size fails (the reference always exits 0, test.cu:120).
 //
 //   bin/test_sgemm --mmin=2 --mmax=3072 --mstep=1 --savedir=test_results
 //                  [--path=plain|bf16x6|tf32x3] [--seed=0] [--dist=u01|upm1|pow2]
@@ -51,8 +53,7 @@ int main(int argc, char** argv) {
         HCHECK(cudaMemcpy(hr.data(), Cref, sizeof(float) * hr.size(), cudaMemcpyDeviceToHost));
         HCHECK(cudaGetLastError());
         CmpResult r = compare_mats(hr.data(), hc.data(), hc.size(), 1e-4f);
-        const bool exact_ok = path != SGEMM_B200_PATH_PLAIN || r.n_bit_exact == (long)hc.size();
-        const bool ok = r.equal && exact_ok;
+        const bool ok = r.equal;
         if (!ok) {
             ++n_failed;
             failed += std::to_string(t) + " ";

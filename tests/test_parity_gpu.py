@@ -74,7 +74,7 @@ def test_plain_bit_exact_vs_oracle(shape, ab):
     alpha, beta = ab
     A, B, C = _inputs(m, n, k, 1, 0)
     got = _run_ours(A, B, C, alpha, beta)
-    want = oracle.sgemm_basic(A, B, C, alpha, beta, read_c_if_beta_zero=False)
+    want = oracle.sgemm_basic(A, B, C, alpha, beta, basic=False)
     _assert_equal(got, want)
 
 
@@ -87,8 +87,14 @@ def test_every_config_bit_exact(cfg, shape):
         pytest.skip("config not built")
     m, n, k = shape
     A, B, C = _inputs(m, n, k, 2, 2)
+    if names[cfg].startswith("tma_") and (k % 4 or n % 4):
+        # TMA needs 16-byte row strides; a forced TMA config must refuse.
+        with pytest.raises(sg.SgemmError) as e:
+            _run_ours(A, B, C, 1.5, 0.5, config=cfg)
+        assert e.value.status == sg.ERR_INVALID_ARG
+        return
     got = _run_ours(A, B, C, 1.5, 0.5, config=cfg)
-    _assert_equal(got, oracle.sgemm_basic(A, B, C, 1.5, 0.5, read_c_if_beta_zero=False))
+    _assert_equal(got, oracle.sgemm_basic(A, B, C, 1.5, 0.5, basic=False))
 
 
 @pytest.mark.parametrize("lds", [(None, None, None), (36, 52, 60), (33, 49, 51), (37, 48, 50)],
@@ -97,7 +103,7 @@ def test_general_strides_and_canaries(lds):
     m, n, k = 45, 47, 33
     A, B, C = _inputs(m, n, k, 3, 0)
     got = _run_ours(A, B, C, 1.5, 0.5, lds=lds)
-    _assert_equal(got, oracle.sgemm_basic(A, B, C, 1.5, 0.5, read_c_if_beta_zero=False))
+    _assert_equal(got, oracle.sgemm_basic(A, B, C, 1.5, 0.5, basic=False))
 
 
 def test_beta_zero_never_reads_c():
@@ -106,7 +112,7 @@ def test_beta_zero_never_reads_c():
     C = np.full((m, n), np.nan, dtype=np.float32)
     got = _run_ours(A, B, C, 1.0, 0.0)
     assert np.isfinite(got).all()
-    _assert_equal(got, oracle.sgemm_basic(A, B, C, 1.0, 0.0, read_c_if_beta_zero=False))
+    _assert_equal(got, oracle.sgemm_basic(A, B, C, 1.0, 0.0, basic=False))
 
 
 def test_k_zero_scales_c():
@@ -123,29 +129,59 @@ def test_k_zero_scales_c():
     _assert_equal(dC.cpu().numpy(), oracle.sgemm_basic(A, B, C, 1.5, 0.5))
 
 
-@pytest.mark.parametrize("size", [1000, 1024, 2600, 3001])
-def test_bit_exact_vs_reference_kernels(size):
+def _device_inputs(m, n, k, seed):
+    torch = _torch()
+    A = torch.empty((m, k), device="cuda")
+    B = torch.empty((k, n), device="cuda")
+    C = torch.empty((m, n), device="cuda")
+    sg.fill_random(A, seed, 1, sg.DIST_UNIFORM_PM1)
+    sg.fill_random(B, seed, 2, sg.DIST_UNIFORM_PM1)
+    sg.fill_random(C, seed, 3, sg.DIST_UNIFORM_PM1)
+    torch.cuda.synchronize()
+    return A, B, C
+
+
+@pytest.mark.parametrize("shape", [(2600, 2600, 2600), (3001, 3001, 3001), (4096, 4096, 4096),
+                                   (2501, 640, 1000)], ids=lambda s: "x".join(map(str, s)))
+def test_bit_exact_vs_reference_128x256x8(shape):
     """Same seeded inputs through the reference's own sgemm() (built from its
     sources for sm_100a) and through ours; ldb == ldc == n as the reference
-    requires.  2600 and 3001 dispatch to sgemm_128x256x8, the others to
-    sgemm_128x128x8."""
+    requires.  With m > 2500 or n > 2500 the reference runs sgemm_128x256x8
+    (src/sgemm.cuh:42-44), whose results ours must equal bit for bit."""
     torch = _torch()
-    m = n = k = size
-    dev = torch.device("cuda")
-    A = torch.empty((m, k), device=dev)
-    B = torch.empty((k, n), device=dev)
-    C = torch.empty((m, n), device=dev)
-    sg.fill_random(A, 6, 1, sg.DIST_UNIFORM_PM1)
-    sg.fill_random(B, 6, 2, sg.DIST_UNIFORM_PM1)
-    sg.fill_random(C, 6, 3, sg.DIST_UNIFORM_PM1)
+    m, n, k = shape
+    assert oracle.ref().ref_sgemm_kernel_choice(m, n) == 1
+    A, B, C = _device_inputs(m, n, k, 6)
     C_ref = C.clone()
+    torch.cuda.synchronize()
     sg.sgemm(A, B, C, 1.5, 0.5)
     oracle.ref_sgemm(A, B, C_ref, 1.5, 0.5)
     torch.cuda.synchronize()
     assert torch.equal(C, C_ref)
 
 
+def test_reference_128x128x8_defect_vs_ours():
+    """Recorded finding: at m, n <= 2500 the reference dispatches
+    sgemm_128x128x8, which built for sm_100a returns wrong values once k > 8
+    (see tests/test_oracle.py::test_reference_128x128x8_defect_on_sm100).
+    Ours must equal the oracle exactly on the same inputs."""
+    torch = _torch()
+    m = n = k = 1000
+    A, B, C = _inputs(m, n, k, 6, 0)
+    dA, dB = torch.from_numpy(A).cuda(), torch.from_numpy(B).cuda()
+    c_ours, c_ref = torch.from_numpy(C).cuda(), torch.from_numpy(C).cuda()
+    sg.sgemm(dA, dB, c_ours, 1.5, 0.5)
+    oracle.ref_sgemm(dA, dB, c_ref, 1.5, 0.5)
+    torch.cuda.synchronize()
+    want = oracle.sgemm_basic(A, B, C, 1.5, 0.5, basic=False)
+    _assert_equal(c_ours.cpu().numpy(), want)
+    ref, mag = oracle.dgemm(A, B, C, 1.5, 0.5)
+    assert oracle.error_stats(c_ref.cpu().numpy(), ref, mag)["max_componentwise"] > 1e-3
+
+
 def test_reference_naive_kernel_matches_ours():
+    """sgemm_b200_basic equals the reference's sgemm_basic()/kernel_basic bit
+    for bit (epilogue fma(acc, alpha, c*beta), C always read)."""
     torch = _torch()
     m, n, k = 77, 91, 129
     A, B, C = _inputs(m, n, k, 7, 0)
@@ -154,8 +190,8 @@ def test_reference_naive_kernel_matches_ours():
     sg.sgemm_basic(dA, dB, c1, 1.5, 0.5)
     oracle.ref_sgemm(dA, dB, c2, 1.5, 0.5, basic=True)
     torch.cuda.synchronize()
+    _assert_equal(c1.cpu().numpy(), oracle.sgemm_basic(A, B, C, 1.5, 0.5, basic=True))
     assert torch.equal(c1, c2)
-    _assert_equal(c1.cpu().numpy(), oracle.sgemm_basic(A, B, C, 1.5, 0.5))
 
 
 def test_device_fill_matches_host_generator():
@@ -186,7 +222,7 @@ def test_large_sizes_sampled_rows(size):
     got = C[torch.from_numpy(rows).long().cuda()].cpu().numpy()
     hA = oracle.fill(m, k, 8, 1, 0)
     hB = oracle.fill(k, n, 8, 2, 0)
-    want = oracle.sgemm_basic_rows(rows, hA, hB, C0_rows, 1.5, 0.5, read_c_if_beta_zero=False)
+    want = oracle.sgemm_basic_rows(rows, hA, hB, C0_rows, 1.5, 0.5, basic=False)
     _assert_equal(got, want)
 
 

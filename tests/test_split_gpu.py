@@ -1,0 +1,153 @@
+"""GPU tests of the split-precision tensor-core paths (BF16x6, TF32x3).
+
+No reference counterpart exists (the reference has no tensor-core path); the
+contract is sgemm()'s (src/sgemm.cuh:19-30).  Accuracy is judged against the
+FP64 oracle with the componentwise metric
+    max |c - c64| / (|alpha| (|A||B|)_ij + |beta| |C0|_ij)
+next to the plain FFMA path's error on the same inputs.
+"""
+import numpy as np
+import pytest
+
+import oracle
+import sgemm_b200 as sg
+
+pytestmark = pytest.mark.gpu
+
+PATHS = ["bf16x6", "tf32x3"]
+
+# Componentwise error bounds (FP32 unit roundoff u = 2^-24 ~ 6e-8).  BF16x6
+# keeps ~24 significant bits per operand (the three dropped products are
+# below 3 * 2^-24 |a||b|); TF32x3 keeps ~22.  Both accumulate in FP32.
+TOL_SMALL_K = {"bf16x6": 8e-7, "tf32x3": 4e-6}
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def _run(path, A, B, C, alpha, beta, ws=True, lds=(None, None, None)):
+    torch = _torch()
+    m, k = A.shape
+    n = B.shape[1]
+
+    def dev(x, ld):
+        rows, cols = x.shape
+        big = torch.full((rows, ld or cols), float("nan"), device="cuda")
+        big[:, :cols] = torch.from_numpy(x).cuda()
+        return big, big[:, :cols]
+
+    bA, dA = dev(A, lds[0])
+    bB, dB = dev(B, lds[1])
+    bC, dC = dev(C, lds[2])
+    work = None
+    if ws:
+        work = torch.empty(sg.split_workspace_size(sg.PATHS[path], m, n, k), dtype=torch.uint8,
+                           device="cuda")
+    sg.sgemm_split(path, dA, dB, dC, alpha, beta, workspace=work)
+    torch.cuda.synchronize()
+    assert sg.device_status() == sg.OK
+    full = bC.cpu().numpy()
+    if lds[2]:
+        assert np.isnan(full[:, n:]).all(), "wrote outside the C tile"
+    return full[:, :n]
+
+
+def _errors(got, A, B, C, alpha, beta):
+    ref, mag = oracle.dgemm(A, B, C, alpha, beta)
+    return oracle.error_stats(got, ref, mag)
+
+
+SHAPES = [(1, 1, 1), (7, 13, 9), (128, 256, 32), (129, 257, 33), (200, 136, 1001),
+          (255, 300, 17), (300, 520, 64), (513, 260, 130)]
+
+
+@pytest.mark.parametrize("path", PATHS)
+@pytest.mark.parametrize("shape", SHAPES, ids=lambda s: "x".join(map(str, s)))
+def test_split_accuracy_small(path, shape):
+    m, n, k = shape
+    A = oracle.fill(m, k, 11, 1, 0)
+    B = oracle.fill(k, n, 11, 2, 0)
+    C = oracle.fill(m, n, 11, 3, 0)
+    got = _run(path, A, B, C, 1.5, 0.5)
+    e = _errors(got, A, B, C, 1.5, 0.5)
+    plain = oracle.sgemm_basic(A, B, C, 1.5, 0.5, basic=False)
+    ep = _errors(plain, A, B, C, 1.5, 0.5)
+    print(f"{path} {shape}: split {e['max_componentwise']:.3e} plain "
+          f"{ep['max_componentwise']:.3e}")
+    assert e["non_finite"] == 0
+    assert e["max_componentwise"] < TOL_SMALL_K[path]
+
+
+@pytest.mark.parametrize("path", PATHS)
+def test_split_pow2_inputs(path):
+    """sign * 2^e * U[1,2), e in [-10, 10]: wide dynamic range."""
+    m, n, k = 260, 300, 512
+    A = oracle.fill(m, k, 12, 1, 2)
+    B = oracle.fill(k, n, 12, 2, 2)
+    C = oracle.fill(m, n, 12, 3, 2)
+    got = _run(path, A, B, C, 1.5, 0.5)
+    e = _errors(got, A, B, C, 1.5, 0.5)
+    print(path, e)
+    assert e["max_componentwise"] < TOL_SMALL_K[path]
+
+
+@pytest.mark.parametrize("path", PATHS)
+def test_split_beta_zero_and_strides(path):
+    m, n, k = 140, 270, 45
+    A = oracle.fill(m, k, 13, 1, 0)
+    B = oracle.fill(k, n, 13, 2, 0)
+    C = np.full((m, n), np.nan, dtype=np.float32)
+    got = _run(path, A, B, C, 1.0, 0.0, lds=(47, 275, 273))
+    assert np.isfinite(got).all()
+    e = _errors(got, A, B, np.zeros_like(C), 1.0, 0.0)
+    assert e["max_componentwise"] < TOL_SMALL_K[path]
+
+
+@pytest.mark.parametrize("path", PATHS)
+def test_split_internal_workspace(path):
+    """workspace=None: the call allocates and frees it stream-ordered."""
+    m, n, k = 300, 200, 100
+    A = oracle.fill(m, k, 14, 1, 0)
+    B = oracle.fill(k, n, 14, 2, 0)
+    C = oracle.fill(m, n, 14, 3, 0)
+    a = _run(path, A, B, C, 1.5, 0.5, ws=True)
+    b = _run(path, A, B, C, 1.5, 0.5, ws=False)
+    assert np.array_equal(a, b)  # deterministic
+
+
+def test_split_workspace_too_small():
+    torch = _torch()
+    A = torch.zeros((64, 64), device="cuda")
+    ws = torch.empty(16, dtype=torch.uint8, device="cuda")
+    with pytest.raises(sg.SgemmError) as e:
+        sg.sgemm_split("bf16x6", A, A, A.clone(), 1.0, 0.0, workspace=ws)
+    assert e.value.status == sg.ERR_NO_MEMORY
+
+
+@pytest.mark.parametrize("dist", [0, 2], ids=["upm1", "pow2"])
+def test_split_8192_error_not_worse_than_plain(dist):
+    """Full 8192^3 on the GPU FP64 oracle: the split paths' componentwise
+    error must not exceed the plain FFMA path's (north-star criterion)."""
+    torch = _torch()
+    n = 8192
+    A = torch.empty((n, n), device="cuda")
+    B = torch.empty((n, n), device="cuda")
+    C0 = torch.empty((n, n), device="cuda")
+    for t, X in ((1, A), (2, B), (3, C0)):
+        sg.fill_random(X, 21, t, dist)
+    results = {}
+    C = C0.clone()
+    sg.sgemm(A, B, C, 1.5, 0.5)
+    results["plain"] = oracle.gpu_error_stats(A, B, C0, C, 1.5, 0.5)
+    for path in PATHS:
+        C = C0.clone()
+        sg.sgemm_split(path, A, B, C, 1.5, 0.5)
+        torch.cuda.synchronize()
+        results[path] = oracle.gpu_error_stats(A, B, C0, C, 1.5, 0.5)
+    for k, v in results.items():
+        print(k, v)
+    for path in PATHS:
+        assert results[path]["non_finite"] == 0
+        assert results[path]["max_componentwise"] <= 2.0 * results["plain"]["max_componentwise"]
