@@ -12,19 +12,30 @@
 // TF32X3: x_h = tf32(x), x_l = tf32(x - x_h);  A*B = hh + (hl + lh).
 //
 // The products run as tcgen05.mma (kind::f16 with BF16 inputs, or
-// kind::tf32) with FP32 accumulation in tensor memory.  The dominant hh term
-// and the small correction terms accumulate in two separate TMEM accumulators
-// (D1, D2) that the epilogue adds once, so the correction sum's rounding is
-// ~2^-8 smaller than the main sum's.
+// kind::tf32) with FP32 accumulation in tensor memory.  Two things keep the
+// result as accurate as the FP32 FFMA path:
+//  - the dominant hh term and the small correction terms accumulate in
+//    separate TMEM accumulators (D1, D2), so the corrections' rounding is
+//    ~2^-8 smaller than the main sum's;
+//  - the tensor core only ever accumulates one K chunk (KCHUNK = 128) into a
+//    TMEM buffer; eight drain warps then add that chunk's D1 + D2 into FP32
+//    registers with round-to-nearest while the MMA warp fills the other
+//    buffer.  Long accumulations inside the tensor core lose accuracy with
+//    K; chunk sums added on the CUDA cores do not.
 //
-// Kernel shape: one CTA of 4 warps per 128 x 256 output tile.
-//   warp 0 / lane 0  TMA producer: one 3-D box per operand per stage brings
-//                    all split planes of a K slice (64-byte rows, 64-byte swizzle)
-//   warp 1 / lane 0  MMA issuer: tcgen05.mma M=128 N=256, commit per stage
-//   warps 0..3       epilogue: tcgen05.ld 32 lanes x 32 columns, alpha/beta,
-//                    float4 stores (warp w owns TMEM lanes / rows 32w..32w+31)
-// Every mbarrier wait is bounded (ptx.cuh); on expiry the status word is set,
-// in-flight copies and MMAs are drained with bounded waits, TMEM is freed.
+// Kernel shape: one CTA of 10 warps per 128 x 128 output tile.
+//   warps 0..7  drain + epilogue: warp w reads TMEM lanes 32*(w%4).. (rows)
+//               and columns 64*(w/4)..+63 of each chunk, keeps 64 FP32
+//               running sums, and finally applies alpha/beta and stores
+//               float4s
+//   warp 8      TMA producer (one lane): one 3-D box per operand per stage
+//               brings every split plane of a 64-byte K slice (64-byte swizzle)
+//   warp 9      MMA issuer (one lane): tcgen05.mma M=128 N=128; commit per
+//               stage frees the stage, commit per chunk hands the chunk's
+//               TMEM buffer to the drain warps
+// TMEM (512 columns): buffer b in {0,1} holds D1 at 256b and D2 at 256b+128.
+// Every mbarrier wait is bounded (ptx.cuh); on expiry the status word is
+// set, in-flight copies are drained with bounded waits and TMEM is freed.
 //
 // A split pre-pass writes the operand planes (A as [split][M][Kp], B
 // transposed to [split][N][Kp], both K-major) into a workspace.
@@ -39,25 +50,32 @@
 namespace sgb {
 namespace split {
 
-constexpr int BM = 128, BN = 256, THREADS = 128;
-constexpr int TMEM_COLS = 512;  // D1 at column 0, D2 at column BN
+constexpr int BM = 128, BN = 128;
+constexpr int DRAIN_WARPS = 8, PRODUCER_WARP = 8, MMA_WARP = 9;
+constexpr int THREADS = 32 * (DRAIN_WARPS + 2);
+constexpr int TMEM_COLS = 512;
+constexpr int KCHUNK = 128;  // K depth one TMEM accumulation spans
 
 template <int PATH>
 struct Traits;
 
 template <>
 struct Traits<SGEMM_B200_PATH_BF16X6> {
-    static constexpr int NSPLIT = 3, ESZ = 2, BK = 32, KMMA = 16, STAGES = 3;
+    static constexpr int NSPLIT = 3, ESZ = 2, BK = 32, KMMA = 16, STAGES = 4;
     static constexpr uint32_t FMT = 1;  // BF16
     static constexpr int NPROD = 6;
-    // (a split, b split, accumulator) in issue order
-    __device__ static constexpr int pa(int i) { return i == 0 ? 0 : (i == 1 || i == 3) ? 0 : (i == 5 ? 1 : (i == 2 ? 1 : 2)); }
-    __device__ static constexpr int pb(int i) { return i == 0 ? 0 : i == 1 ? 1 : i == 2 ? 0 : i == 3 ? 2 : i == 4 ? 0 : 1; }
+    // (a split, b split) in issue order: hh first (D1), then the corrections (D2)
+    __device__ static constexpr int pa(int i) {
+        return i == 0 ? 0 : i == 1 ? 0 : i == 2 ? 1 : i == 3 ? 0 : i == 4 ? 2 : 1;
+    }
+    __device__ static constexpr int pb(int i) {
+        return i == 0 ? 0 : i == 1 ? 1 : i == 2 ? 0 : i == 3 ? 2 : i == 4 ? 0 : 1;
+    }
 };
 
 template <>
 struct Traits<SGEMM_B200_PATH_TF32X3> {
-    static constexpr int NSPLIT = 2, ESZ = 4, BK = 16, KMMA = 8, STAGES = 4;
+    static constexpr int NSPLIT = 2, ESZ = 4, BK = 16, KMMA = 8, STAGES = 6;
     static constexpr uint32_t FMT = 2;  // TF32
     static constexpr int NPROD = 3;
     __device__ static constexpr int pa(int i) { return i == 2 ? 1 : 0; }
@@ -70,11 +88,13 @@ struct Layout {
     static constexpr int ROW_BYTES = T::BK * T::ESZ;  // 64: one swizzle-64 row
     static_assert(ROW_BYTES == 64, "64-byte K rows");
     static constexpr int A_PLANE = BM * ROW_BYTES;    // 8 KB
-    static constexpr int B_PLANE = BN * ROW_BYTES;    // 16 KB
+    static constexpr int B_PLANE = BN * ROW_BYTES;    // 8 KB
     static constexpr int A_BYTES = T::NSPLIT * A_PLANE;
     static constexpr int B_BYTES = T::NSPLIT * B_PLANE;
     static constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
     static constexpr int SMEM_BYTES = T::STAGES * STAGE_BYTES + 1024;
+    static constexpr int CHUNK_STAGES = KCHUNK / T::BK;
+    static_assert(KCHUNK % T::BK == 0, "whole stages per chunk");
     static_assert(SMEM_BYTES <= 227 * 1024, "shared memory budget");
 };
 
@@ -108,7 +128,8 @@ __global__ void __launch_bounds__(THREADS, 1)
     extern __shared__ uint8_t smem_raw[];
     __shared__ __align__(8) uint64_t full_bar[T::STAGES];
     __shared__ __align__(8) uint64_t empty_bar[T::STAGES];
-    __shared__ __align__(8) uint64_t done_bar;
+    __shared__ __align__(8) uint64_t filled_bar[2];
+    __shared__ __align__(8) uint64_t drained_bar[2];
     __shared__ uint32_t tmem_base_s;
     __shared__ volatile int abort_s;
     __shared__ int consumed_s;
@@ -120,18 +141,20 @@ __global__ void __launch_bounds__(THREADS, 1)
     tile_coords(blockIdx.x, p.tiles_m, p.tiles_n, tm, tn);
     const int m0 = tm * BM, n0 = tn * BN;
     const int nk = (p.k + T::BK - 1) / T::BK;
+    const int nchunks = (nk + L::CHUNK_STAGES - 1) / L::CHUNK_STAGES;
 
     if (tid == 0) {
         for (int s = 0; s < T::STAGES; ++s) {
             mbar_init(&full_bar[s], 1);
             mbar_init(&empty_bar[s], 1);
         }
-        mbar_init(&done_bar, 1);
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(&filled_bar[b], 1);
+            mbar_init(&drained_bar[b], DRAIN_WARPS);
+        }
         abort_s = 0;
         consumed_s = 0;
         fence_barrier_init();
-        tma_prefetch_desc(&tmA);
-        tma_prefetch_desc(&tmB);
     }
     if (warp == 0) {
         tmem_alloc(&tmem_base_s, TMEM_COLS);
@@ -143,93 +166,127 @@ __global__ void __launch_bounds__(THREADS, 1)
     const uint32_t tmem = tmem_base_s;
 
     int issued = 0;
-    if (warp == 0 && lane == 0) {
-        // ---------------------------------------------------- TMA producer --
-        for (int kb = 0; kb < nk; ++kb) {
-            const int s = kb % T::STAGES;
-            if (kb >= T::STAGES) {
-                if (!mbar_wait(&empty_bar[s], ((kb / T::STAGES) - 1) & 1) || abort_s) {
-                    abort_s = 1;
-                    atomicExch(p.status, SGEMM_B200_ERR_TIMEOUT);
+    float acc[64];
+    if (warp == PRODUCER_WARP) {
+        if (lane == 0) {
+            // ------------------------------------------------ TMA producer --
+            tma_prefetch_desc(&tmA);
+            tma_prefetch_desc(&tmB);
+            for (int kb = 0; kb < nk; ++kb) {
+                const int s = kb % T::STAGES;
+                if (kb >= T::STAGES) {
+                    if (!mbar_wait(&empty_bar[s], ((kb / T::STAGES) - 1) & 1) || abort_s) {
+                        abort_s = 1;
+                        atomicExch(p.status, SGEMM_B200_ERR_TIMEOUT);
+                        break;
+                    }
+                }
+                uint8_t* st = smem + s * L::STAGE_BYTES;
+                mbar_arrive_expect_tx(&full_bar[s], L::STAGE_BYTES);
+                tma_load_3d(st, &tmA, &full_bar[s], kb * T::BK, m0, 0);
+                tma_load_3d(st + L::A_BYTES, &tmB, &full_bar[s], kb * T::BK, n0, 0);
+                ++issued;
+            }
+        }
+    } else if (warp == MMA_WARP) {
+        if (lane == 0) {
+            // -------------------------------------------------- MMA issuer --
+            constexpr uint32_t idesc = make_idesc(T::FMT, BM, BN);
+            int kb = 0;
+            bool ok = true;
+            for (int c = 0; c < nchunks && ok; ++c) {
+                const int b = c & 1;
+                if (c >= 2 && (!mbar_wait(&drained_bar[b], ((c >> 1) - 1) & 1) || abort_s)) {
+                    ok = false;
                     break;
                 }
+                tc_fence_after();
+                const uint32_t d1 = tmem + static_cast<uint32_t>(b * 256);
+                const int kend = min(nk, (c + 1) * L::CHUNK_STAGES);
+                for (; kb < kend; ++kb) {
+                    const int s = kb % T::STAGES;
+                    if (!mbar_wait(&full_bar[s], (kb / T::STAGES) & 1) || abort_s) {
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t a0 = smem_u32(smem + s * L::STAGE_BYTES);
+                    const uint32_t b0 = a0 + L::A_BYTES;
+                    const bool chunk_start = kb == c * L::CHUNK_STAGES;
+#pragma unroll
+                    for (int j = 0; j < T::BK / T::KMMA; ++j) {
+                        const uint32_t koff = j * T::KMMA * T::ESZ;  // 32 B per MMA K slice
+#pragma unroll
+                        for (int i = 0; i < T::NPROD; ++i) {
+                            const uint64_t ad =
+                                sw64_kmajor_desc(a0 + T::pa(i) * L::A_PLANE + koff);
+                            const uint64_t bd =
+                                sw64_kmajor_desc(b0 + T::pb(i) * L::B_PLANE + koff);
+                            const uint32_t d = d1 + (i == 0 ? 0u : static_cast<uint32_t>(BN));
+                            // the first product into each accumulator of a chunk overwrites it
+                            const uint32_t accum = (chunk_start && j == 0 && i <= 1) ? 0u : 1u;
+                            if constexpr (T::FMT == 1)
+                                mma_bf16_ss(d, ad, bd, idesc, accum);
+                            else
+                                mma_tf32_ss(d, ad, bd, idesc, accum);
+                        }
+                    }
+                    mma_commit(&empty_bar[s]);  // frees the stage once these MMAs read it
+                }
+                if (!ok) break;
+                mma_commit(&filled_bar[b]);  // the chunk's sums are ready in buffer b
             }
-            uint8_t* st = smem + s * L::STAGE_BYTES;
-            mbar_arrive_expect_tx(&full_bar[s], L::STAGE_BYTES);
-            tma_load_3d(st, &tmA, &full_bar[s], kb * T::BK, m0, 0);
-            tma_load_3d(st + L::A_BYTES, &tmB, &full_bar[s], kb * T::BK, n0, 0);
-            ++issued;
-        }
-    } else if (warp == 1 && lane == 0) {
-        // ------------------------------------------------------ MMA issuer --
-        constexpr uint32_t idesc = make_idesc(T::FMT, BM, BN);
-        int kb = 0;
-        for (; kb < nk; ++kb) {
-            const int s = kb % T::STAGES;
-            if (!mbar_wait(&full_bar[s], (kb / T::STAGES) & 1) || abort_s) {
+            if (!ok) {
                 abort_s = 1;
                 atomicExch(p.status, SGEMM_B200_ERR_TIMEOUT);
+            }
+            consumed_s = kb;
+        }
+    } else {
+        // ------------------------------------------------ drain + epilogue --
+        const int q = warp & 3, h = warp >> 2;
+        const uint32_t trow = tmem + (static_cast<uint32_t>(q * 32) << 16) + h * 64;
+#pragma unroll
+        for (int j = 0; j < 64; ++j) acc[j] = 0.0f;
+        bool ok = true;
+        for (int c = 0; c < nchunks; ++c) {
+            const int b = c & 1;
+            if (!mbar_wait(&filled_bar[b], (c >> 1) & 1) || abort_s) {
+                ok = false;
                 break;
             }
             tc_fence_after();
-            const uint32_t a0 = smem_u32(smem + s * L::STAGE_BYTES);
-            const uint32_t b0 = a0 + L::A_BYTES;
 #pragma unroll
-            for (int j = 0; j < T::BK / T::KMMA; ++j) {
-                const uint32_t koff = j * T::KMMA * T::ESZ;  // 32 bytes per MMA K slice
-#pragma unroll
-                for (int i = 0; i < T::NPROD; ++i) {
-                    const uint64_t ad = sw64_kmajor_desc(a0 + T::pa(i) * L::A_PLANE + koff);
-                    const uint64_t bd = sw64_kmajor_desc(b0 + T::pb(i) * L::B_PLANE + koff);
-                    const uint32_t d = tmem + (i == 0 ? 0u : static_cast<uint32_t>(BN));
-                    // first product into each accumulator overwrites it
-                    const uint32_t acc = (kb > 0 || j > 0 || (i > 1)) ? 1u : 0u;
-                    if constexpr (T::FMT == 1)
-                        mma_bf16_ss(d, ad, bd, idesc, acc);
-                    else
-                        mma_tf32_ss(d, ad, bd, idesc, acc);
-                }
-            }
-            mma_commit(&empty_bar[s]);  // frees the stage once these MMAs read it
-        }
-        consumed_s = kb;
-        mma_commit(&done_bar);  // arrives when every MMA issued above has completed
-    }
-
-    // ------------------------------------------------------------ epilogue --
-    __syncwarp();
-    bool ok = nk == 0 ? true : mbar_wait(&done_bar, 0);
-    if (!ok) atomicExch(p.status, SGEMM_B200_ERR_TIMEOUT);
-    ok = ok && !abort_s;
-    tc_fence_after();
-
-    const int row = m0 + warp * 32 + lane;
-    const uint32_t trow = tmem + (static_cast<uint32_t>(warp * 32) << 16);
-    if (ok) {
-        for (int c = 0; c < BN / 32; ++c) {
-            const int col0 = n0 + c * 32;
-            if (col0 >= p.n) break;  // uniform across the warp
-            uint32_t d1[32], d2[32];
-            if (nk > 0) {
-                tmem_ld_32x32b_x32(trow + c * 32, d1);
-                tmem_ld_32x32b_x32(trow + BN + c * 32, d2);
+            for (int g = 0; g < 2; ++g) {
+                uint32_t r1[32], r2[32];
+                tmem_ld_32x32b_x32(trow + b * 256 + g * 32, r1);
+                tmem_ld_32x32b_x32(trow + b * 256 + BN + g * 32, r2);
                 tmem_ld_wait();
-            } else {
-#pragma unroll
-                for (int j = 0; j < 32; ++j) d1[j] = d2[j] = 0u;
-            }
-            if (row < p.m) {
-                float* crow = p.C + (int64_t)row * p.ldc + col0;
-                float v[32];
 #pragma unroll
                 for (int j = 0; j < 32; ++j)
-                    v[j] = __fmul_rn(__fadd_rn(__uint_as_float(d1[j]), __uint_as_float(d2[j])),
-                                     p.alpha);
-                if (p.vec_c && col0 + 31 < p.n) {
+                    acc[g * 32 + j] = __fadd_rn(
+                        acc[g * 32 + j], __fadd_rn(__uint_as_float(r1[j]), __uint_as_float(r2[j])));
+            }
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&drained_bar[b]);
+        }
+        if (!ok) {
+            abort_s = 1;
+            atomicExch(p.status, SGEMM_B200_ERR_TIMEOUT);
+        } else if (!abort_s) {
+            const int row = m0 + q * 32 + lane;
+            const int col0 = n0 + h * 64;
+            if (row < p.m && col0 < p.n) {
+                float* crow = p.C + (int64_t)row * p.ldc + col0;
+                if (p.vec_c && col0 + 63 < p.n) {
 #pragma unroll
-                    for (int q = 0; q < 8; ++q) {
-                        float4* dst = reinterpret_cast<float4*>(crow + 4 * q);
-                        float4 o = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+                    for (int v = 0; v < 16; ++v) {
+                        float4 o = make_float4(__fmul_rn(acc[4 * v], p.alpha),
+                                               __fmul_rn(acc[4 * v + 1], p.alpha),
+                                               __fmul_rn(acc[4 * v + 2], p.alpha),
+                                               __fmul_rn(acc[4 * v + 3], p.alpha));
+                        float4* dst = reinterpret_cast<float4*>(crow + 4 * v);
                         if (p.beta != 0.0f) {
                             const float4 old = *dst;
                             o.x = fmaf(old.x, p.beta, o.x);
@@ -241,9 +298,9 @@ __global__ void __launch_bounds__(THREADS, 1)
                     }
                 } else {
 #pragma unroll
-                    for (int j = 0; j < 32; ++j) {
+                    for (int j = 0; j < 64; ++j) {
                         if (col0 + j < p.n) {
-                            float o = v[j];
+                            float o = __fmul_rn(acc[j], p.alpha);
                             if (p.beta != 0.0f) o = fmaf(crow[j], p.beta, o);
                             crow[j] = o;
                         }
@@ -255,14 +312,14 @@ __global__ void __launch_bounds__(THREADS, 1)
 
     // ------------------------------------------------------------ teardown --
     tc_fence_before();
-    __syncthreads();  // every TMEM load is done; consumed_s is visible
+    __syncthreads();  // every TMEM load and MMA is done; consumed_s is visible
+    if (warp == PRODUCER_WARP && lane == 0) {
+        // Copies the MMA issuer never consumed (only after an abort) must land
+        // before this CTA's shared memory is released.
+        for (int j = consumed_s; j < issued; ++j)
+            if (!mbar_wait(&full_bar[j % T::STAGES], (j / T::STAGES) & 1)) break;
+    }
     if (warp == 0) {
-        if (lane == 0) {
-            // Copies the MMA issuer never consumed (only after an abort) must
-            // land before this CTA's shared memory is released.
-            for (int j = consumed_s; j < issued; ++j)
-                if (!mbar_wait(&full_bar[j % T::STAGES], (j / T::STAGES) & 1)) break;
-        }
         __syncwarp();
         tmem_dealloc(tmem, TMEM_COLS);
     }

@@ -16,10 +16,16 @@ pytestmark = pytest.mark.gpu
 
 PATHS = ["bf16x6", "tf32x3"]
 
-# Componentwise error bounds (FP32 unit roundoff u = 2^-24 ~ 6e-8).  BF16x6
-# keeps ~24 significant bits per operand (the three dropped products are
-# below 3 * 2^-24 |a||b|); TF32x3 keeps ~22.  Both accumulate in FP32.
-TOL_SMALL_K = {"bf16x6": 8e-7, "tf32x3": 4e-6}
+# Small shapes: the split path's componentwise error must stay within
+# 1.5x the plain FFMA path's on the same inputs, plus one FP32 ulp (2^-23)
+# of slack for the rounding of the final alpha/beta step.  BF16x6 keeps ~24
+# significant bits per operand (the three dropped products are below
+# 3 * 2^-24 |a||b|); TF32x3 keeps ~22.
+ULP = 2.0 ** -23
+
+
+def _bound(plain_err):
+    return 1.5 * plain_err + ULP
 
 
 def _torch():
@@ -77,7 +83,7 @@ def test_split_accuracy_small(path, shape):
     print(f"{path} {shape}: split {e['max_componentwise']:.3e} plain "
           f"{ep['max_componentwise']:.3e}")
     assert e["non_finite"] == 0
-    assert e["max_componentwise"] < TOL_SMALL_K[path]
+    assert e["max_componentwise"] <= _bound(ep["max_componentwise"])
 
 
 @pytest.mark.parametrize("path", PATHS)
@@ -89,8 +95,9 @@ def test_split_pow2_inputs(path):
     C = oracle.fill(m, n, 12, 3, 2)
     got = _run(path, A, B, C, 1.5, 0.5)
     e = _errors(got, A, B, C, 1.5, 0.5)
-    print(path, e)
-    assert e["max_componentwise"] < TOL_SMALL_K[path]
+    ep = _errors(oracle.sgemm_basic(A, B, C, 1.5, 0.5, basic=False), A, B, C, 1.5, 0.5)
+    print(path, e, ep)
+    assert e["max_componentwise"] <= _bound(ep["max_componentwise"])
 
 
 @pytest.mark.parametrize("path", PATHS)
@@ -101,8 +108,10 @@ def test_split_beta_zero_and_strides(path):
     C = np.full((m, n), np.nan, dtype=np.float32)
     got = _run(path, A, B, C, 1.0, 0.0, lds=(47, 275, 273))
     assert np.isfinite(got).all()
-    e = _errors(got, A, B, np.zeros_like(C), 1.0, 0.0)
-    assert e["max_componentwise"] < TOL_SMALL_K[path]
+    Z = np.zeros_like(C)
+    e = _errors(got, A, B, Z, 1.0, 0.0)
+    ep = _errors(oracle.sgemm_basic(A, B, Z, 1.0, 0.0, basic=False), A, B, Z, 1.0, 0.0)
+    assert e["max_componentwise"] <= _bound(ep["max_componentwise"])
 
 
 @pytest.mark.parametrize("path", PATHS)
@@ -128,8 +137,8 @@ def test_split_workspace_too_small():
 
 @pytest.mark.parametrize("dist", [0, 2], ids=["upm1", "pow2"])
 def test_split_8192_error_not_worse_than_plain(dist):
-    """Full 8192^3 on the GPU FP64 oracle: the split paths' componentwise
-    error must not exceed the plain FFMA path's (north-star criterion)."""
+    """Full 8192^3 on the GPU FP64 oracle: the split paths' error (max
+    componentwise and mean relative) must not exceed the plain FFMA path's."""
     torch = _torch()
     n = 8192
     A = torch.empty((n, n), device="cuda")
@@ -150,4 +159,5 @@ def test_split_8192_error_not_worse_than_plain(dist):
         print(k, v)
     for path in PATHS:
         assert results[path]["non_finite"] == 0
-        assert results[path]["max_componentwise"] <= 2.0 * results["plain"]["max_componentwise"]
+        assert results[path]["max_componentwise"] <= results["plain"]["max_componentwise"]
+        assert results[path]["mean_rel"] <= results["plain"]["mean_rel"]
