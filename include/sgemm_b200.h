@@ -162,9 +162,25 @@ int sgemm_b200_grouped_plan_info(const sgemm_b200_grouped_plan* plan,
                                  int* tiles, int* work_items, int* grid_ctas);
 void sgemm_b200_grouped_plan_destroy(sgemm_b200_grouped_plan* plan);
 
-/* One-shot convenience: plan, launch once, destroy. */
+/* One-shot convenience: plan, launch once, synchronise, destroy. */
 int sgemm_b200_grouped(const sgemm_b200_problem* problems, int count,
                        sgemm_b200_stream_t stream);
+
+/* The baseline the grouped launch replaces: one sgemm_b200 call per problem,
+ * in order, on `stream`. */
+int sgemm_b200_grouped_sequential(const sgemm_b200_problem* problems, int count,
+                                  sgemm_b200_stream_t stream);
+
+/* Host-only schedule summary (no device needed): the tiles, work items and
+ * split-K workspace bytes a plan for these problems would use with the given
+ * tuning table (NULL = built-in choices, or when the table does not match). */
+int sgemm_b200_grouped_schedule(const sgemm_b200_problem* problems, int count,
+                                const char* tuning_json, int* tiles, int* work_items,
+                                size_t* workspace_bytes);
+
+/* Size bucket (0..8) the tuning table keys a problem by: 3 classes of M*N
+ * (< 256^2, < 1024^2, larger) x 3 classes of K (< 512, < 2048, larger). */
+int sgemm_b200_grouped_bucket(int m, int n, int k);
 
 /* Time the candidate tile/stage/split-K choices per size bucket on the current
  * device with the given problems and write the winners to json_path. */

@@ -126,22 +126,22 @@ int plain_launch(int cfg, int m, int n, int k, float alpha, const float* A, int 
         return SGEMM_B200_ERR_INVALID_ARG;
 
     Params p;
-    p.m = m;
-    p.n = n;
-    p.k = k;
-    p.lda = lda;
-    p.ldb = ldb;
-    p.ldc = ldc;
-    p.alpha = alpha;
-    p.beta = beta;
-    p.A = A;
-    p.B = B;
-    p.C = C;
+    p.op.m = m;
+    p.op.n = n;
+    p.op.k = k;
+    p.op.lda = lda;
+    p.op.ldb = ldb;
+    p.op.ldc = ldc;
+    p.op.alpha = alpha;
+    p.op.beta = beta;
+    p.op.A = A;
+    p.op.B = B;
+    p.op.C = C;
+    p.op.vec_c = (ldc % 4 == 0) && (reinterpret_cast<uintptr_t>(C) % 16 == 0);
     p.status = device_status_ptr();
     if (!p.status) return SGEMM_B200_ERR_CUDA;
     p.tiles_m = div_up(m, cd.bm);
     p.tiles_n = div_up(n, cd.bn);
-    p.vec_c = (ldc % 4 == 0) && (reinterpret_cast<uintptr_t>(C) % 16 == 0);
 
     CUtensorMap tmA, tmB;
     std::memset(&tmA, 0, sizeof(tmA));

@@ -52,17 +52,6 @@ struct Cfg {
     static constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024;  // + alignment slack
 };
 
-struct Params {
-    int m, n, k;
-    int lda, ldb, ldc;
-    float alpha, beta;
-    const float* A;
-    const float* B;
-    float* C;
-    int* status;
-    int tiles_m, tiles_n;
-    int vec_c;  // C rows are 16-byte aligned (ldc % 4 == 0 and C aligned)
-};
 
 // Grouped rasterisation: 8 tile-rows share a band so concurrently resident
 // CTAs reuse A rows and B columns out of L2.
@@ -114,10 +103,22 @@ __device__ __forceinline__ void compute_stage(const uint8_t* __restrict__ As,
     }
 }
 
+// Operand and output views of one GEMM, shared by the single-problem kernel
+// and the grouped persistent kernel.
+struct Operands {
+    int m, n, k;
+    int lda, ldb, ldc;
+    float alpha, beta;
+    const float* A;
+    const float* B;
+    float* C;
+    int vec_c;
+};
+
 // cp.async loader for one k block (any stride, any alignment).
 template <class C>
-__device__ __forceinline__ void load_stage_async4(const Params& p, uint8_t* As, uint8_t* Bs, int m0,
-                                                  int n0, int k0, int tid) {
+__device__ __forceinline__ void load_stage_async4(const Operands& p, uint8_t* As, uint8_t* Bs,
+                                                  int m0, int n0, int k0, int tid) {
     const uint32_t as = smem_u32(As), bs = smem_u32(Bs);
     constexpr int A_ELEMS = C::BM * C::BK;
 #pragma unroll 4
@@ -138,9 +139,11 @@ __device__ __forceinline__ void load_stage_async4(const Params& p, uint8_t* As, 
     }
 }
 
+// Thread (wm, wn, lm, ln) owns rows m0 + 32wm + lm + 4i (i < 8) and the float4
+// column groups n0 + wn*8*TN + 4ln + 32g (g < TN/4).
 template <class C>
-__device__ __forceinline__ void epilogue(const Params& p, int m0, int n0, int wm, int wn, int lm,
-                                         int ln, float (&acc)[C::TM][C::TN]) {
+__device__ __forceinline__ void epilogue(const Operands& p, int m0, int n0, int wm, int wn, int lm,
+                                         int ln, const float (&acc)[C::TM][C::TN]) {
     const int col0 = n0 + wn * 8 * C::TN + ln * 4;
 #pragma unroll
     for (int i = 0; i < C::TM; ++i) {
@@ -177,6 +180,12 @@ __device__ __forceinline__ void epilogue(const Params& p, int m0, int n0, int wm
     }
 }
 
+struct Params {
+    Operands op;  // vec_c: C rows are 16-byte aligned (ldc % 4 == 0 and C aligned)
+    int* status;
+    int tiles_m, tiles_n;
+};
+
 template <class C>
 __global__ void __launch_bounds__(C::THREADS, C::MINB)
     ffma_gemm_kernel(const __grid_constant__ CUtensorMap tmA,
@@ -194,7 +203,7 @@ __global__ void __launch_bounds__(C::THREADS, C::MINB)
     int tm, tn;
     tile_coords(blockIdx.x, p.tiles_m, p.tiles_n, tm, tn);
     const int m0 = tm * C::BM, n0 = tn * C::BN;
-    const int nk = (p.k + C::BK - 1) / C::BK;
+    const int nk = (p.op.k + C::BK - 1) / C::BK;
 
     // Per-thread shared-memory offsets (bytes within a stage).
     const uint32_t a_base = static_cast<uint32_t>((wm * 32 + lm) * 128);
@@ -258,7 +267,7 @@ __global__ void __launch_bounds__(C::THREADS, C::MINB)
         for (int s = 0; s < C::STAGES - 1; ++s) {
             if (s < nk) {
                 uint8_t* st = smem + s * C::STAGE_BYTES;
-                load_stage_async4<C>(p, st, st + C::A_BYTES, m0, n0, s * C::BK, tid);
+                load_stage_async4<C>(p.op, st, st + C::A_BYTES, m0, n0, s * C::BK, tid);
             }
             cp_async_commit();
         }
@@ -268,7 +277,7 @@ __global__ void __launch_bounds__(C::THREADS, C::MINB)
             const int nxt = kb + C::STAGES - 1;
             if (nxt < nk) {
                 uint8_t* st = smem + (nxt % C::STAGES) * C::STAGE_BYTES;
-                load_stage_async4<C>(p, st, st + C::A_BYTES, m0, n0, nxt * C::BK, tid);
+                load_stage_async4<C>(p.op, st, st + C::A_BYTES, m0, n0, nxt * C::BK, tid);
             }
             cp_async_commit();
             const uint8_t* st = smem + (kb % C::STAGES) * C::STAGE_BYTES;
@@ -277,7 +286,7 @@ __global__ void __launch_bounds__(C::THREADS, C::MINB)
         cp_async_wait<0>();
     }
 
-    epilogue<C>(p, m0, n0, wm, wn, lm, ln, acc);
+    epilogue<C>(p.op, m0, n0, wm, wn, lm, ln, acc);
 }
 
 }  // namespace ffma
