@@ -192,8 +192,7 @@ __global__ void __launch_bounds__(C::THREADS, C::MINB)
                      const __grid_constant__ CUtensorMap tmB, const Params p) {
     extern __shared__ uint8_t smem_raw[];
     __shared__ __align__(8) uint64_t full_bar[C::STAGES];
-    uint8_t* smem = reinterpret_cast<uint8_t*>(
-        (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
+    uint8_t* smem = align_smem_1024(smem_raw);
 
     const int tid = threadIdx.x;
     const int warp = tid >> 5, lane = tid & 31;

@@ -225,8 +225,7 @@ __global__ void __launch_bounds__(THREADS, 1) grouped_kernel(const GParams gp) {
     __shared__ __align__(8) uint64_t full_bar[S];
     __shared__ int item_s;
     __shared__ int last_s;
-    uint8_t* smem = reinterpret_cast<uint8_t*>(
-        (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
+    uint8_t* smem = align_smem_1024(smem_raw);
     const int tid = threadIdx.x;
     if (tid == 0) {
         for (int s = 0; s < S; ++s) mbar_init(&full_bar[s], 1);

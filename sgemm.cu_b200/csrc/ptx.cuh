@@ -26,6 +26,15 @@ __device__ __forceinline__ uint32_t smem_u32(const void* p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
 
+// First 1024-byte aligned byte of a dynamic shared-memory array.  The offset
+// is added to the array pointer itself (not computed through an integer
+// cast) so the compiler still knows the result points to shared memory and
+// emits shared loads (LDS) rather than generic ones.
+__device__ __forceinline__ uint8_t* align_smem_1024(uint8_t* smem_raw) {
+    const uint32_t pad = (1024u - (smem_u32(smem_raw) & 1023u)) & 1023u;
+    return smem_raw + pad;
+}
+
 __device__ __forceinline__ uint64_t globaltimer_ns() {
     uint64_t t;
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));

@@ -133,8 +133,7 @@ __global__ void __launch_bounds__(THREADS, 1)
     __shared__ uint32_t tmem_base_s;
     __shared__ volatile int abort_s;
     __shared__ int consumed_s;
-    uint8_t* smem = reinterpret_cast<uint8_t*>(
-        (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
+    uint8_t* smem = align_smem_1024(smem_raw);
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     int tm, tn;

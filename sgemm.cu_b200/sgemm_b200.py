@@ -85,6 +85,11 @@ def _declare(lib: ctypes.CDLL) -> None:
       [_P, ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(_I)])
     d("sgemm_b200_grouped_plan_destroy", None, [_P])
     d("sgemm_b200_grouped", _I, [ctypes.POINTER(Problem), _I, _P])
+    d("sgemm_b200_grouped_sequential", _I, [ctypes.POINTER(Problem), _I, _P])
+    d("sgemm_b200_grouped_schedule", _I,
+      [ctypes.POINTER(Problem), _I, ctypes.c_char_p, ctypes.POINTER(_I), ctypes.POINTER(_I),
+       ctypes.POINTER(ctypes.c_size_t)])
+    d("sgemm_b200_grouped_bucket", _I, [_I, _I, _I])
     d("sgemm_b200_autotune_grouped", _I, [ctypes.POINTER(Problem), _I, ctypes.c_char_p])
     d("sgemm_b200_fill_random", _I, [_P, _I, _I, _I, ctypes.c_uint64, ctypes.c_uint32, _I, _P])
     d("sgemm_b200_device_status", _I, [])
@@ -231,12 +236,47 @@ def make_problems(specs: Sequence) -> "ctypes.Array":
     return arr
 
 
+def grouped_sequential(problems, stream=None) -> None:
+    """The baseline: one plain sgemm_b200 launch per problem, in order."""
+    _check(lib().sgemm_b200_grouped_sequential(problems, len(problems), _stream_ptr(stream)),
+           "grouped_sequential")
+
+
+def grouped_schedule(problems, tuning_json: Optional[str] = None) -> dict:
+    """Host-only schedule summary (tiles, work items, split-K workspace bytes)."""
+    t, w, b = ctypes.c_int(), ctypes.c_int(), ctypes.c_size_t()
+    _check(lib().sgemm_b200_grouped_schedule(problems, len(problems),
+                                             tuning_json.encode() if tuning_json else None,
+                                             ctypes.byref(t), ctypes.byref(w), ctypes.byref(b)),
+           "grouped_schedule")
+    return {"tiles": t.value, "work_items": w.value, "workspace_bytes": b.value}
+
+
+def grouped_bucket(m: int, n: int, k: int) -> int:
+    return lib().sgemm_b200_grouped_bucket(m, n, k)
+
+
+def autotune_grouped(problems, json_path: str) -> None:
+    """Time tile/split-K/stage candidates per size bucket on these problems
+    (their C matrices are overwritten) and write the winners to json_path."""
+    _check(lib().sgemm_b200_autotune_grouped(problems, len(problems), json_path.encode()),
+           "autotune_grouped")
+
+
+def host_problems(shapes) -> "ctypes.Array":
+    """Problem table with placeholder pointers (for host-only schedule queries)."""
+    arr = (Problem * len(shapes))()
+    for i, (m, n, k) in enumerate(shapes):
+        arr[i] = Problem(m, n, k, max(k, 1), max(n, 1), max(n, 1), 1.0, 0.0, 256, 256, 256)
+    return arr
+
+
 class GroupedPlan:
     """Persistent grouped GEMM over a fixed list of problems."""
 
     def __init__(self, specs: Sequence, tuning_json: Optional[str] = None):
         self._problems = make_problems(specs)
-        self._keep = specs  # keep tensors alive
+        self._keep = list(specs)  # keep tensors alive
         h = ctypes.c_void_p()
         _check(lib().sgemm_b200_grouped_plan_create(
             ctypes.byref(h), self._problems, len(specs),

@@ -1,0 +1,44 @@
+"""CPU tests of the grouped GEMM's host-side scheduling (no GPU)."""
+import math
+
+import pytest
+
+import sgemm_b200 as sg
+
+
+def test_bucket_classes():
+    assert sg.grouped_bucket(64, 64, 64) == 0
+    assert sg.grouped_bucket(64, 64, 4096) == 2
+    assert sg.grouped_bucket(512, 512, 1000) == 4
+    assert sg.grouped_bucket(4096, 4096, 4096) == 8
+    assert sg.grouped_bucket(1024, 512, 100) == 3
+    assert sg.grouped_bucket(2048, 512, 100) == 6
+
+
+def test_schedule_default_counts():
+    shapes = [(64, 64, 64), (300, 520, 1001), (4096, 4096, 64), (1, 1, 1), (129, 257, 0)]
+    probs = sg.host_problems(shapes)
+    s = sg.grouped_schedule(probs)
+    tiles = 0
+    for m, n, k in shapes:
+        bn = 256 if m * n >= 1024 * 1024 else 128  # default: 128x256 only for the largest class
+        tiles += math.ceil(m / 128) * math.ceil(n / bn)
+    assert s["tiles"] == tiles
+    assert s["work_items"] == tiles  # no split-K by default: results equal the plain path
+    assert s["workspace_bytes"] == 0
+
+
+def test_schedule_ignores_table_for_other_device(tmp_path):
+    p = tmp_path / "t.json"
+    p.write_text('{\n "device": "Some Other GPU",\n "sm_count": 7,\n "stages": 3,\n'
+                 ' "buckets": [\n  {"mn": 0, "k": 2, "tile": 1, "split": 4}\n ]\n}\n')
+    probs = sg.host_problems([(64, 64, 4096)])
+    assert sg.grouped_schedule(probs, str(p))["work_items"] == 1
+
+
+def test_schedule_rejects_bad_problem():
+    probs = sg.host_problems([(64, 64, 64)])
+    probs[0].ldc = 3
+    with pytest.raises(sg.SgemmError) as e:
+        sg.grouped_schedule(probs)
+    assert e.value.status == sg.ERR_INVALID_ARG
