@@ -34,6 +34,7 @@
 
 #include "common.h"
 #include "ffma_kernel.cuh"
+#include "grouped.h"
 #include "plain.h"
 
 namespace sgb {
@@ -572,6 +573,101 @@ static int launch(sgemm_b200_grouped_plan* plan, cudaStream_t stream, int use_gr
         if (e != cudaSuccess) return cuda_status(e);
     }
     return cuda_status(cudaGraphLaunch(plan->exec, stream));
+}
+
+// ------------------------------------------------------------ arena path --
+// Batch launcher for the serving loop: device buffers and pinned staging
+// buffers are allocated once and grown on demand, so a batch costs a host
+// schedule, a few async copies and one kernel launch (no cudaMalloc, no
+// graph capture).  An arena must not be reused before its previous batch
+// completed (the staging buffers feed async copies).
+
+template <class T>
+static cudaError_t grow(T** d, T** h, size_t* cap, size_t need, cudaStream_t s) {
+    if (need <= *cap) return cudaSuccess;
+    const size_t n = std::max(need, *cap * 2);
+    if (*d) cudaFreeAsync(*d, s);
+    *d = nullptr;
+    if (h && *h) {
+        cudaFreeHost(*h);
+        *h = nullptr;
+    }
+    cudaError_t e = cudaMallocAsync(reinterpret_cast<void**>(d), n * sizeof(T), s);
+    if (e == cudaSuccess && h) e = cudaMallocHost(reinterpret_cast<void**>(h), n * sizeof(T));
+    if (e == cudaSuccess) *cap = n;
+    return e;
+}
+
+int arena_launch(Arena* a, const sgemm_b200_problem* probs, int count, cudaStream_t stream) {
+    if (!device_is_sm100()) return SGEMM_B200_ERR_UNSUPPORTED;
+    Table table;  // built-in choices: split-K off, so results equal the plain path's
+    Schedule sc;
+    const int st = make_schedule(probs, count, table, &sc);
+    if (st != SGEMM_B200_OK) return st;
+    if (sc.items.empty()) return SGEMM_B200_OK;
+    cudaError_t e = cudaSuccess;
+    auto chk = [&](cudaError_t x) {
+        if (e == cudaSuccess) e = x;
+    };
+    const size_t n_counters = 1 + (size_t)sc.tickets;
+    chk(grow(&a->d_probs, &a->h_probs, &a->cap_probs, (size_t)count, stream));
+    chk(grow(&a->d_items, &a->h_items, &a->cap_items, sc.items.size(), stream));
+    chk(grow(&a->d_maps, &a->h_maps, &a->cap_maps, 2 * (size_t)count, stream));
+    chk(grow<int>(&a->d_counters, nullptr, &a->cap_counters, n_counters, stream));
+    chk(grow<float>(&a->d_ws, nullptr, &a->cap_ws, std::max<size_t>(sc.ws_floats, 1), stream));
+    if (e != cudaSuccess) return cuda_status(e);
+    std::memcpy(a->h_probs, sc.probs.data(), sizeof(GProblem) * count);
+    std::memcpy(a->h_items, sc.items.data(), sizeof(GItem) * sc.items.size());
+    std::memset(a->h_maps, 0, sizeof(CUtensorMap) * 2 * count);
+    for (int i = 0; i < count; ++i) {
+        const GProblem& g = sc.probs[i];
+        if (!g.tma) continue;
+        const int bn = g.tile == kTileL ? 256 : 128;
+        if (!encode_tensor_map_2d(&a->h_maps[2 * i], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, g.op.A,
+                                  (uint64_t)g.op.k, (uint64_t)g.op.m, (uint64_t)g.op.lda * 4, 32,
+                                  128, CU_TENSOR_MAP_SWIZZLE_128B) ||
+            !encode_tensor_map_2d(&a->h_maps[2 * i + 1], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, g.op.B,
+                                  (uint64_t)g.op.n, (uint64_t)g.op.k, (uint64_t)g.op.ldb * 4, bn,
+                                  32, CU_TENSOR_MAP_SWIZZLE_NONE))
+            return SGEMM_B200_ERR_CUDA;
+    }
+    chk(cudaMemcpyAsync(a->d_probs, a->h_probs, sizeof(GProblem) * count, cudaMemcpyHostToDevice,
+                        stream));
+    chk(cudaMemcpyAsync(a->d_items, a->h_items, sizeof(GItem) * sc.items.size(),
+                        cudaMemcpyHostToDevice, stream));
+    chk(cudaMemcpyAsync(a->d_maps, a->h_maps, sizeof(CUtensorMap) * 2 * count,
+                        cudaMemcpyHostToDevice, stream));
+    chk(cudaMemsetAsync(a->d_counters, 0, sizeof(int) * n_counters, stream));
+    if (e != cudaSuccess) return cuda_status(e);
+    static bool attrs = false;
+    if (!attrs) {
+        set_kernel_attributes();
+        attrs = true;
+    }
+    GParams p;
+    p.probs = a->d_probs;
+    p.items = a->d_items;
+    p.maps = a->d_maps;
+    p.ws = a->d_ws;
+    p.counters = a->d_counters;
+    p.status = device_status_ptr();
+    p.n_items = (int)sc.items.size();
+    if (!p.status) return SGEMM_B200_ERR_CUDA;
+    const int grid = std::max(1, std::min(device_info().sm_count, p.n_items));
+    grouped_kernel<4><<<grid, THREADS, smem_bytes<4>(), stream>>>(p);
+    return cuda_status(cudaGetLastError());
+}
+
+void arena_release(Arena* a) {
+    cudaFree(a->d_probs);
+    cudaFree(a->d_items);
+    cudaFree(a->d_maps);
+    cudaFree(a->d_counters);
+    cudaFree(a->d_ws);
+    cudaFreeHost(a->h_probs);
+    cudaFreeHost(a->h_items);
+    cudaFreeHost(a->h_maps);
+    *a = Arena();
 }
 
 // Median device time (ms) of `reps` graph launches of a plan.
