@@ -121,6 +121,36 @@ int sgemm_b200_split(int path, int m, int n, int k,
                      void* workspace, size_t workspace_bytes,
                      sgemm_b200_stream_t stream);
 
+/* Allocation-free split-precision GEMM.  No counterpart in the reference
+ * (which never allocates, and has no split path).
+ *
+ * For callers that must not allocate device memory during a call: code that
+ * runs where another component owns the device allocator (a framework that
+ * reserved the GPU's memory up front), latency-critical loops in which
+ * cudaMalloc/cudaFree would synchronise the device, and fixed-footprint
+ * deployments that must not fail for lack of memory at run time.
+ *
+ * Same arguments and result as sgemm_b200_split, but the split operand planes
+ * go to one static 64 MiB device array inside this library instead of a
+ * workspace: the call makes no cudaMalloc, cudaFree or other allocation.  The
+ * array exists on every GPU that loads this library until the process exits.
+ * Problems whose planes need more than 64 MiB
+ * (sgemm_b200_split_workspace_size(path, m, n, k) > 64 MiB, e.g. BF16X6
+ * beyond about m = n = k = 2048) are refused with SGEMM_B200_ERR_NO_MEMORY.
+ * The first call on each device looks up the array's device address (with
+ * that device current); make that first call before any stream capture.
+ * Every call shares the one array, so calls whose work overlaps on the GPU
+ * (different streams, or different host threads) race: order them on one
+ * stream.  Nothing in the array needs clearing between calls; each call
+ * rewrites all of the planes it reads. */
+int sgemm_b200_split_noalloc(int path, int m, int n, int k,
+                             const float* alpha,
+                             const float* A, int lda,
+                             const float* B, int ldb,
+                             const float* beta,
+                             float* C, int ldc,
+                             sgemm_b200_stream_t stream);
+
 /* Dispatch by path: PLAIN goes to sgemm_b200, the others to sgemm_b200_split
  * with a stream-ordered workspace. */
 int sgemm_b200_gemm(int path, int m, int n, int k,

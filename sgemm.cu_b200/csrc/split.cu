@@ -42,6 +42,7 @@
 #include <cuda_bf16.h>
 
 #include <cstring>
+#include <mutex>
 
 #include "common.h"
 #include "plain.h"
@@ -561,4 +562,65 @@ extern "C" int sgemm_b200_gemm(int path, int m, int n, int k, const float* alpha
         return sgemm_b200(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, stream);
     return sgemm_b200_split(path, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, nullptr, 0,
                             stream);
+}
+
+// ------------------------------------------------------- allocation-free variant --
+//
+// sgemm_b200_split_noalloc: the split-precision GEMM for callers that may not
+// allocate device memory.  Its scratch (the BF16 / TF32 operand planes the
+// pre-pass writes) is a file-scope static device array of kNoAllocScratchBytes,
+// so the call itself never allocates.  The array is created when this
+// library's device code is loaded on a GPU and stays until the process exits.
+namespace sgb {
+namespace noalloc {
+
+constexpr size_t kNoAllocScratchBytes = size_t(64) << 20;  // 64 MiB per GPU
+static __device__ __align__(256) uint8_t g_split_scratch[kNoAllocScratchBytes];
+
+constexpr int kMaxDevices = 64;
+
+// Device address of the scratch array on the current device, resolved once
+// per device (host code cannot use the array's name as a device address).
+static void* scratch_address(int* status) {
+    static void* addr[kMaxDevices] = {nullptr};
+    static std::mutex mu;
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+        *status = SGEMM_B200_ERR_CUDA;
+        return nullptr;
+    }
+    std::lock_guard<std::mutex> lock(mu);
+    if (!addr[dev]) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_split_scratch);
+        if (e != cudaSuccess || !p) {
+            *status = cuda_status(e == cudaSuccess ? cudaErrorInvalidSymbol : e);
+            return nullptr;
+        }
+        addr[dev] = p;
+    }
+    *status = SGEMM_B200_OK;
+    return addr[dev];
+}
+
+}  // namespace noalloc
+}  // namespace sgb
+
+extern "C" int sgemm_b200_split_noalloc(int path, int m, int n, int k, const float* alpha,
+                                        const float* A, int lda, const float* B, int ldb,
+                                        const float* beta, float* C, int ldc,
+                                        sgemm_b200_stream_t stream) {
+    int s = sgb::check_gemm_args(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+    if (s == SGEMM_B200_OK && path != SGEMM_B200_PATH_BF16X6 && path != SGEMM_B200_PATH_TF32X3)
+        s = SGEMM_B200_ERR_INVALID_ARG;
+    if (s == SGEMM_B200_OK && m > 0 && n > 0 && k > 0 &&
+        sgemm_b200_split_workspace_size(path, m, n, k) > sgb::noalloc::kNoAllocScratchBytes)
+        s = SGEMM_B200_ERR_NO_MEMORY;  // the fixed scratch cannot hold this problem's planes
+    void* scratch = nullptr;
+    if (s == SGEMM_B200_OK) scratch = sgb::noalloc::scratch_address(&s);
+    if (s == SGEMM_B200_OK)
+        s = sgb::split_launch(path, m, n, k, *alpha, A, lda, B, ldb, *beta, C, ldc, scratch,
+                              sgb::noalloc::kNoAllocScratchBytes, sgb::as_stream(stream));
+    sgb::set_last_status(s);
+    return s;
 }
