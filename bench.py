@@ -295,6 +295,94 @@ def _split_leg(torch, sg, A, B, C0, flush, steps, warmup, rows, host_ab, peaks):
     return out
 
 
+def _grouped_workload(n, seed):
+    """512 problems, M, N, K log-uniform on [64, 4096], multiples of 8."""
+    rng = np.random.default_rng(seed)
+    vals = np.exp(rng.uniform(np.log(64), np.log(4096), size=(n, 3)))
+    return [tuple(int(max(8, round(v / 8) * 8)) for v in row) for row in vals]
+
+
+def _grouped_leg(torch, sg, sms, sm_mhz):
+    """One persistent graph-captured launch over 512 uneven problems vs 512
+    sequential plain launches; then the autotuned plan."""
+    shapes = _grouped_workload(512, 7)
+    specs = []
+    for i, (m, n, k) in enumerate(shapes):
+        A = torch.empty((m, k), device="cuda")
+        B = torch.empty((k, n), device="cuda")
+        C = torch.empty((m, n), device="cuda")
+        sg.fill_random(A, 500 + i, 1, 0)
+        sg.fill_random(B, 500 + i, 2, 0)
+        sg.fill_random(C, 500 + i, 3, 0)
+        specs.append((A, B, C, 1.5, 0.5))
+    probs = sg.make_problems(specs)
+    flop = sum(2.0 * m * n * k for m, n, k in shapes)
+
+    def timed(fn, reps):
+        fn()
+        torch.cuda.synchronize()
+        out = []
+        for _ in range(reps):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            fn()
+            b.record()
+            torch.cuda.synchronize()
+            out.append(a.elapsed_time(b))
+        return statistics.median(out)
+
+    plan = sg.GroupedPlan(specs)
+    t_grouped = timed(lambda: plan.launch(use_graph=True), 7)
+    info = plan.info()
+    plan.close()
+    t_seq = timed(lambda: sg.grouped_sequential(probs), 5)
+    tuned = os.path.join("/tmp", f"sgemm_b200_grouped_tuning_{os.getpid()}.json")
+    t0 = time.time()
+    sg.autotune_grouped(probs, tuned)
+    tune_s = time.time() - t0
+    plan = sg.GroupedPlan(specs, tuning_json=tuned)
+    t_tuned = timed(lambda: plan.launch(use_graph=True), 7)
+    tinfo = plan.info()
+    plan.close()
+    with open(tuned) as f:
+        table = json.load(f)
+    os.unlink(tuned)
+    peak = sms * 256 * sm_mhz * 1e-3  # GFLOP/s
+    best = min(t_grouped, t_tuned)
+    return {
+        "workload": "512 problems, M,N,K log-uniform [64,4096] multiples of 8, alpha=1.5 "
+                    "beta=0.5, uniform[-1,1)",
+        "tflop": round(flop * 1e-12, 4),
+        "grouped_ms": round(t_grouped, 3), "grouped_gflops": round(flop / t_grouped * 1e-6, 1),
+        "grouped_tuned_ms": round(t_tuned, 3),
+        "grouped_tuned_gflops": round(flop / t_tuned * 1e-6, 1),
+        "sequential_ms": round(t_seq, 3), "sequential_gflops": round(flop / t_seq * 1e-6, 1),
+        "speedup_vs_sequential": round(t_seq / best, 3),
+        "frac_of_simt_peak": round(flop / best * 1e-6 / peak, 4),
+        "launches": 1, "tiles": info["tiles"], "work_items_default": info["work_items"],
+        "work_items_tuned": tinfo["work_items"], "autotune_s": round(tune_s, 1),
+        "tuning": table,
+    }
+
+
+def _serving_leg(sg, rates, n_requests):
+    out = {"workload": "Poisson arrivals; 60% M~U[16,256] N=K=4096, 40% M=N=K log-uniform "
+                       "[512,4096]; operands generated and resident on the device; 64 GB "
+                       "budget; 2 slots, max batch 32", "runs": []}
+    for path in ("plain", "bf16x6"):
+        for rate in rates:
+            srv = sg.Server(64 << 30, slots=2, max_batch=32, path=path)
+            st = srv.run_poisson(rate, n_requests, seed=11)
+            srv.close()
+            out["runs"].append({
+                "path": path, "rate_per_s": rate, "requests": n_requests,
+                "completed": st["completed"], "p50_ms": round(st["p50_ms"], 3),
+                "p99_ms": round(st["p99_ms"], 3), "gflops": round(st["gflops"], 1),
+                "batches": st["batches"], "max_batch": st["max_batch_size"],
+                "max_batches_in_flight": st["max_batches_in_flight"]})
+    return out
+
+
 # --------------------------------------------------------------------- main --
 
 def run(args):
@@ -400,6 +488,13 @@ def run(args):
         result["split"] = _split_leg(torch, sg, A, B, C0, flush, max(3, args.steps // 2),
                                      args.warmup, np.linspace(0, SIZE - 1, 64).astype(np.int32),
                                      host_ab, peaks)
+    if rank == 0 and world == 1 and not args.skip_grouped:
+        del A, B, C, C0, flush
+        torch.cuda.empty_cache()
+        result["grouped"] = _grouped_leg(torch, sg, sms, sm_max)
+        torch.cuda.empty_cache()
+    if rank == 0 and world == 1 and not args.skip_serving:
+        result["serving"] = _serving_leg(sg, [500.0, 1000.0, 2000.0, 4000.0], 300)
     if rank == 0:
         print(json.dumps(result))
     if dist is not None:
@@ -469,6 +564,8 @@ def main():
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-split", action="store_true")
     ap.add_argument("--skip-e2e", action="store_true")
+    ap.add_argument("--skip-grouped", action="store_true")
+    ap.add_argument("--skip-serving", action="store_true")
     ap.add_argument("--size", type=int, default=SIZE,
                     help="M=N=K (default 8192; smaller sizes only for profiler captures)")
     args = ap.parse_args()

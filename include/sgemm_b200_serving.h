@@ -75,9 +75,11 @@ int sgemm_b200_server_drain(sgemm_b200_server* server);
  * pointer of its C (row stride n), valid until released. */
 int sgemm_b200_server_result(sgemm_b200_server* server, int64_t request_id, double* latency_ms,
                              const float** C, int* ldc, int* batch_size);
+/* Copy a completed request's C (m x n, row-major, packed) to host memory. */
+int sgemm_b200_server_read_result(sgemm_b200_server* server, int64_t request_id, float* host_out);
 int sgemm_b200_server_release(sgemm_b200_server* server, int64_t request_id);
 
-int sgemm_b200_server_stats(sgemm_b200_server* server, sgemm_b200_server_stats* out);
+int sgemm_b200_server_get_stats(sgemm_b200_server* server, sgemm_b200_server_stats* out);
 
 /* Open-loop load: `n_requests` requests with exponential inter-arrival times
  * of mean 1/rate_per_s; 60% tall-skinny (M uniform in [16, 256], N = K =

@@ -1,0 +1,609 @@
+// serving.cu — continuous-batching GEMM server (no reference counterpart; the
+// reference has no serving code).  See include/sgemm_b200_serving.h for the
+// contract.
+//
+// Threads and streams:
+//  - the caller's thread submits requests (or run_poisson submits them on an
+//    open-loop schedule);
+//  - one worker thread admits requests in arrival order while their operands
+//    fit in the pool (generating them on an ingest stream), forms a batch
+//    whenever one of `slots` streams is free, and launches it: one persistent
+//    grouped kernel (plain path) or one split GEMM per request (split paths),
+//    followed by a host callback;
+//  - the callback (a CUDA driver thread; it calls no CUDA API) stamps the
+//    completion time of the batch's requests and hands the slot back.
+// Requests that arrive while batches run are admitted as memory frees and
+// join the next batch; with two or more slots, batches overlap on the GPU.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <condition_variable>
+#include <deque>
+#include <map>
+#include <mutex>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/sgemm_b200_serving.h"
+#include "common.h"
+#include "grouped.h"
+#include "rng.h"
+
+// ------------------------------------------------------------------- pool --
+
+// First-fit offset allocator with coalescing over [0, capacity); 256-byte
+// granularity.  Pure host bookkeeping: the server maps offsets onto one
+// device allocation.
+struct sgemm_b200_pool {
+    size_t capacity = 0;
+    size_t used = 0;
+    std::map<size_t, size_t> free_;  // offset -> size
+    std::map<size_t, size_t> live_;  // offset -> size
+};
+
+namespace sgb {
+namespace serving {
+
+constexpr size_t kAlign = 256;
+
+static size_t round_up(size_t x) { return (x + kAlign - 1) / kAlign * kAlign; }
+
+static int64_t pool_alloc(sgemm_b200_pool* p, size_t bytes) {
+    const size_t need = round_up(std::max<size_t>(bytes, 1));
+    for (auto it = p->free_.begin(); it != p->free_.end(); ++it) {
+        if (it->second < need) continue;
+        const size_t off = it->first, size = it->second;
+        p->free_.erase(it);
+        if (size > need) p->free_[off + need] = size - need;
+        p->live_[off] = need;
+        p->used += need;
+        return (int64_t)off;
+    }
+    return -1;
+}
+
+static int pool_free(sgemm_b200_pool* p, int64_t offset) {
+    auto it = p->live_.find((size_t)offset);
+    if (it == p->live_.end()) return SGEMM_B200_ERR_INVALID_ARG;
+    size_t off = it->first, size = it->second;
+    p->live_.erase(it);
+    p->used -= size;
+    auto next = p->free_.lower_bound(off);
+    if (next != p->free_.end() && off + size == next->first) {
+        size += next->second;
+        next = p->free_.erase(next);
+    }
+    if (next != p->free_.begin()) {
+        auto prev = std::prev(next);
+        if (prev->first + prev->second == off) {
+            prev->second += size;
+            return SGEMM_B200_OK;
+        }
+    }
+    p->free_[off] = size;
+    return SGEMM_B200_OK;
+}
+
+// ---------------------------------------------------------------- workload --
+
+// Uniform double in [0, 1) from the counter-based generator.
+static double unit(uint64_t key, uint64_t i) {
+    return (double)(rng_mix(key + i) >> 11) * (1.0 / 9007199254740992.0);
+}
+
+static void workload(int n, double rate, uint64_t seed, int* mnk, double* gaps) {
+    const uint64_t key = rng_key(seed, 0x5e4u);
+    for (int i = 0; i < n; ++i) {
+        const double u0 = unit(key, 4ull * i), u1 = unit(key, 4ull * i + 1);
+        const double u2 = unit(key, 4ull * i + 2), u3 = unit(key, 4ull * i + 3);
+        if (u0 < 0.6) {  // tall-skinny: M uniform in [16, 256], N = K = 4096
+            mnk[3 * i] = 16 + (int)std::floor(u1 * 241.0);
+            mnk[3 * i + 1] = 4096;
+            mnk[3 * i + 2] = 4096;
+        } else {  // square: log-uniform in [512, 4096], multiple of 8
+            const double s = std::exp(std::log(512.0) + u1 * (std::log(4096.0) - std::log(512.0)));
+            const int v = std::max(512, std::min(4096, (int)std::lround(s / 8.0) * 8));
+            mnk[3 * i] = mnk[3 * i + 1] = mnk[3 * i + 2] = v;
+        }
+        (void)u2;
+        gaps[i] = rate > 0 ? -std::log(1.0 - u3) / rate : 0.0;  // exponential inter-arrival
+    }
+}
+
+// ------------------------------------------------------------------ server --
+
+using Clock = std::chrono::steady_clock;
+
+static double secs(Clock::time_point t) {
+    return std::chrono::duration<double>(t.time_since_epoch()).count();
+}
+
+enum ReqState { kWaiting, kAdmitted, kRunning, kDone, kRejected, kFailed };
+
+struct Request {
+    int64_t id = 0;
+    int m = 0, n = 0, k = 0;
+    float alpha = 1, beta = 0;
+    uint64_t seed = 0;
+    size_t bytes = 0, ws_bytes = 0;
+    int64_t off = -1;
+    float *A = nullptr, *B = nullptr, *C = nullptr;
+    void* ws = nullptr;
+    double t_submit = 0, t_done = 0;
+    int state = kWaiting;
+    int batch_size = 0;
+    bool auto_release = false;
+    cudaEvent_t ready = nullptr;
+};
+
+struct Slot {
+    cudaStream_t stream = nullptr;
+    bool busy = false;
+    std::vector<Request*> batch;
+    grouped::Arena arena;
+};
+
+struct Server;
+
+struct DoneCtx {
+    Server* server;
+    int slot;
+};
+
+struct Server {
+    sgemm_b200_server_config cfg;
+    uint8_t* d_pool = nullptr;
+    sgemm_b200_pool pool;
+    cudaStream_t ingest = nullptr;
+    std::vector<Slot> slots;
+    std::vector<DoneCtx> ctx;
+    int device = 0;
+
+    std::mutex mu;
+    std::condition_variable cv, cv_drain;
+    std::deque<Request*> arrivals;
+    std::deque<Request*> ready;
+    std::deque<int> finished_slots;
+    std::unordered_map<int64_t, Request*> all;
+    std::thread worker;
+    bool stop = false;
+    int64_t next_id = 1;
+    int64_t outstanding = 0;  // submitted and not yet done / rejected / failed
+    int64_t admissions = 0;
+
+    // stats
+    std::vector<double> latencies_ms;
+    double flops_done = 0, t_first_submit = -1, t_last_done = 0;
+    int64_t submitted = 0, completed = 0, rejected = 0, failed = 0, batches = 0;
+    int in_flight = 0, max_in_flight = 0, max_batch_seen = 0;
+    size_t peak_pool = 0;
+    int64_t peak_waiting = 0;
+};
+
+static void CUDART_CB on_batch_done(void* p) {
+    DoneCtx* c = static_cast<DoneCtx*>(p);
+    Server* s = c->server;
+    const double t = secs(Clock::now());
+    std::lock_guard<std::mutex> lock(s->mu);
+    for (Request* r : s->slots[c->slot].batch) r->t_done = t;
+    s->finished_slots.push_back(c->slot);
+    s->cv.notify_all();
+}
+
+static size_t request_bytes(int path, int m, int n, int k, size_t* ws) {
+    const size_t a = round_up((size_t)m * k * 4), b = round_up((size_t)k * n * 4),
+                 c = round_up((size_t)m * n * 4);
+    *ws = path == SGEMM_B200_PATH_PLAIN ? 0
+                                        : round_up(sgemm_b200_split_workspace_size(path, m, n, k));
+    return a + b + c + *ws;
+}
+
+// Called with the lock held.
+static void finish_slot(Server* s, int si) {
+    Slot& sl = s->slots[si];
+    for (Request* r : sl.batch) {
+        r->state = kDone;
+        s->latencies_ms.push_back((r->t_done - r->t_submit) * 1e3);
+        s->flops_done += 2.0 * r->m * (double)r->n * r->k;
+        s->t_last_done = std::max(s->t_last_done, r->t_done);
+        ++s->completed;
+        --s->outstanding;
+        if (r->ready) {
+            cudaEventDestroy(r->ready);
+            r->ready = nullptr;
+        }
+        if (r->auto_release) {
+            pool_free(&s->pool, r->off);
+            r->off = -1;
+        }
+    }
+    sl.batch.clear();
+    sl.busy = false;
+    --s->in_flight;
+}
+
+// Admit arrivals in order while they fit (called with the lock held).
+static void admit(Server* s) {
+    while (!s->arrivals.empty()) {
+        Request* r = s->arrivals.front();
+        int64_t off = -1;
+        const bool injected = s->cfg.inject_alloc_failure_every > 0 &&
+                              (s->admissions + 1) % s->cfg.inject_alloc_failure_every == 0;
+        if (!injected) off = pool_alloc(&s->pool, r->bytes);
+        if (injected) {
+            // An allocation failure the pool could not recover from: refuse.
+            ++s->admissions;
+            s->arrivals.pop_front();
+            r->state = kFailed;
+            ++s->failed;
+            --s->outstanding;
+            continue;
+        }
+        if (off < 0) break;  // wait for memory to free (keeps arrival order)
+        ++s->admissions;
+        s->arrivals.pop_front();
+        r->off = off;
+        uint8_t* base = s->d_pool + off;
+        const size_t a = round_up((size_t)r->m * r->k * 4), b = round_up((size_t)r->k * r->n * 4),
+                     c = round_up((size_t)r->m * r->n * 4);
+        r->A = reinterpret_cast<float*>(base);
+        r->B = reinterpret_cast<float*>(base + a);
+        r->C = reinterpret_cast<float*>(base + a + b);
+        r->ws = r->ws_bytes ? base + a + b + c : nullptr;
+        s->peak_pool = std::max(s->peak_pool, s->pool.used);
+        // Operands arrive: generated on the device, resident from here on.
+        sgemm_b200_fill_random(r->A, r->m, r->k, r->k, r->seed, 1, SGEMM_B200_DIST_UNIFORM_PM1,
+                               s->ingest);
+        sgemm_b200_fill_random(r->B, r->k, r->n, r->n, r->seed, 2, SGEMM_B200_DIST_UNIFORM_PM1,
+                               s->ingest);
+        sgemm_b200_fill_random(r->C, r->m, r->n, r->n, r->seed, 3, SGEMM_B200_DIST_UNIFORM_PM1,
+                               s->ingest);
+        cudaEventCreateWithFlags(&r->ready, cudaEventDisableTiming);
+        cudaEventRecord(r->ready, s->ingest);
+        r->state = kAdmitted;
+        s->ready.push_back(r);
+    }
+}
+
+static int launch_batch(Server* s, int si) {
+    Slot& sl = s->slots[si];
+    if (s->cfg.inject_batch_delay_ms > 0)
+        std::this_thread::sleep_for(std::chrono::milliseconds(s->cfg.inject_batch_delay_ms));
+    for (Request* r : sl.batch) cudaStreamWaitEvent(sl.stream, r->ready, 0);
+    int st = SGEMM_B200_OK;
+    if (s->cfg.path == SGEMM_B200_PATH_PLAIN) {
+        std::vector<sgemm_b200_problem> probs(sl.batch.size());
+        for (size_t i = 0; i < sl.batch.size(); ++i) {
+            const Request* r = sl.batch[i];
+            probs[i] = sgemm_b200_problem{r->m, r->n, r->k, r->k, r->n, r->n, r->alpha,
+                                          r->beta, r->A, r->B, r->C};
+        }
+        st = grouped::arena_launch(&sl.arena, probs.data(), (int)probs.size(), sl.stream);
+    } else {
+        for (Request* r : sl.batch) {
+            st = sgemm_b200_split(s->cfg.path, r->m, r->n, r->k, &r->alpha, r->A, r->k, r->B,
+                                  r->n, &r->beta, r->C, r->n, r->ws, r->ws_bytes, sl.stream);
+            if (st != SGEMM_B200_OK) break;
+        }
+    }
+    if (st == SGEMM_B200_OK)
+        st = cuda_status(cudaLaunchHostFunc(sl.stream, on_batch_done, &s->ctx[si]));
+    return st;
+}
+
+static void worker_loop(Server* s) {
+    cudaSetDevice(s->device);
+    std::unique_lock<std::mutex> lock(s->mu);
+    while (true) {
+        while (!s->finished_slots.empty()) {
+            const int si = s->finished_slots.front();
+            s->finished_slots.pop_front();
+            finish_slot(s, si);
+        }
+        admit(s);
+        s->peak_waiting = std::max<int64_t>(s->peak_waiting, (int64_t)s->arrivals.size());
+        int free_slot = -1;
+        for (size_t i = 0; i < s->slots.size(); ++i)
+            if (!s->slots[i].busy) {
+                free_slot = (int)i;
+                break;
+            }
+        if (free_slot >= 0 && !s->ready.empty()) {
+            Slot& sl = s->slots[free_slot];
+            while (!s->ready.empty() && (int)sl.batch.size() < s->cfg.max_batch) {
+                Request* r = s->ready.front();
+                s->ready.pop_front();
+                r->state = kRunning;
+                sl.batch.push_back(r);
+            }
+            for (Request* r : sl.batch) r->batch_size = (int)sl.batch.size();
+            sl.busy = true;
+            ++s->in_flight;
+            ++s->batches;
+            s->max_in_flight = std::max(s->max_in_flight, s->in_flight);
+            s->max_batch_seen = std::max(s->max_batch_seen, (int)sl.batch.size());
+            lock.unlock();
+            const int st = launch_batch(s, free_slot);
+            lock.lock();
+            if (st != SGEMM_B200_OK) {
+                // The batch never reached the GPU: fail its requests.
+                for (Request* r : sl.batch) {
+                    r->state = kFailed;
+                    ++s->failed;
+                    --s->outstanding;
+                    if (r->auto_release) {
+                        pool_free(&s->pool, r->off);
+                        r->off = -1;
+                    }
+                }
+                sl.batch.clear();
+                sl.busy = false;
+                --s->in_flight;
+            }
+            continue;
+        }
+        if (s->outstanding == 0) s->cv_drain.notify_all();
+        if (s->stop && s->outstanding == 0) break;
+        s->cv.wait_for(lock, std::chrono::milliseconds(2));
+    }
+}
+
+}  // namespace serving
+}  // namespace sgb
+
+struct sgemm_b200_server {
+    sgb::serving::Server s;
+};
+
+using sgb::serving::Request;
+using sgb::serving::Server;
+
+extern "C" sgemm_b200_pool* sgemm_b200_pool_create(size_t capacity) {
+    auto* p = new sgemm_b200_pool();
+    p->capacity = capacity / sgb::serving::kAlign * sgb::serving::kAlign;
+    if (p->capacity) p->free_[0] = p->capacity;
+    return p;
+}
+extern "C" void sgemm_b200_pool_destroy(sgemm_b200_pool* p) { delete p; }
+extern "C" int64_t sgemm_b200_pool_alloc(sgemm_b200_pool* p, size_t bytes) {
+    return p ? sgb::serving::pool_alloc(p, bytes) : -1;
+}
+extern "C" int sgemm_b200_pool_free(sgemm_b200_pool* p, int64_t off) {
+    return p ? sgb::serving::pool_free(p, off) : SGEMM_B200_ERR_INVALID_ARG;
+}
+extern "C" size_t sgemm_b200_pool_used(const sgemm_b200_pool* p) { return p ? p->used : 0; }
+extern "C" size_t sgemm_b200_pool_largest_free(const sgemm_b200_pool* p) {
+    size_t best = 0;
+    if (p)
+        for (const auto& kv : p->free_) best = std::max(best, kv.second);
+    return best;
+}
+
+extern "C" int sgemm_b200_serving_workload(int n_requests, double rate, uint64_t seed, int* mnk,
+                                           double* gaps) {
+    if (n_requests < 0 || !mnk || !gaps || rate < 0) return SGEMM_B200_ERR_INVALID_ARG;
+    sgb::serving::workload(n_requests, rate, seed, mnk, gaps);
+    return SGEMM_B200_OK;
+}
+
+extern "C" int sgemm_b200_server_create(sgemm_b200_server** out,
+                                        const sgemm_b200_server_config* cfg) {
+    if (!out || !cfg || cfg->slots < 1 || cfg->max_batch < 1 || cfg->hbm_budget_bytes == 0 ||
+        cfg->path < 0 || cfg->path > 2)
+        return SGEMM_B200_ERR_INVALID_ARG;
+    if (!sgb::device_is_sm100()) return SGEMM_B200_ERR_UNSUPPORTED;
+    auto* srv = new sgemm_b200_server();
+    Server* s = &srv->s;
+    s->cfg = *cfg;
+    cudaGetDevice(&s->device);
+    s->pool.capacity = cfg->hbm_budget_bytes / sgb::serving::kAlign * sgb::serving::kAlign;
+    s->pool.free_[0] = s->pool.capacity;
+    cudaError_t e = cudaMalloc(&s->d_pool, s->pool.capacity);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->ingest, cudaStreamNonBlocking);
+    s->slots.resize(cfg->slots);
+    s->ctx.resize(cfg->slots);
+    for (int i = 0; i < cfg->slots && e == cudaSuccess; ++i) {
+        e = cudaStreamCreateWithFlags(&s->slots[i].stream, cudaStreamNonBlocking);
+        s->ctx[i] = sgb::serving::DoneCtx{s, i};
+    }
+    if (e != cudaSuccess) {
+        for (auto& sl : s->slots)
+            if (sl.stream) cudaStreamDestroy(sl.stream);
+        if (s->ingest) cudaStreamDestroy(s->ingest);
+        cudaFree(s->d_pool);
+        delete srv;
+        return sgb::cuda_status(e);
+    }
+    s->worker = std::thread(sgb::serving::worker_loop, s);
+    *out = srv;
+    return SGEMM_B200_OK;
+}
+
+extern "C" int sgemm_b200_server_submit(sgemm_b200_server* srv, int m, int n, int k, float alpha,
+                                        float beta, uint64_t seed, int64_t* id) {
+    if (!srv || m <= 0 || n <= 0 || k <= 0) return SGEMM_B200_ERR_INVALID_ARG;
+    Server* s = &srv->s;
+    auto* r = new Request();
+    r->m = m;
+    r->n = n;
+    r->k = k;
+    r->alpha = alpha;
+    r->beta = beta;
+    r->seed = seed;
+    r->bytes = sgb::serving::request_bytes(s->cfg.path, m, n, k, &r->ws_bytes);
+    r->t_submit = sgb::serving::secs(sgb::serving::Clock::now());
+    r->auto_release = s->cfg.keep_results == 0;
+    std::lock_guard<std::mutex> lock(s->mu);
+    r->id = s->next_id++;
+    s->all[r->id] = r;
+    if (id) *id = r->id;
+    ++s->submitted;
+    if (s->t_first_submit < 0) s->t_first_submit = r->t_submit;
+    if (r->bytes > s->pool.capacity) {  // could never fit: refuse now
+        r->state = sgb::serving::kRejected;
+        ++s->rejected;
+        return SGEMM_B200_ERR_REJECTED;
+    }
+    ++s->outstanding;
+    s->arrivals.push_back(r);
+    s->cv.notify_all();
+    return SGEMM_B200_OK;
+}
+
+extern "C" int sgemm_b200_server_drain(sgemm_b200_server* srv) {
+    if (!srv) return SGEMM_B200_ERR_INVALID_ARG;
+    Server* s = &srv->s;
+    std::unique_lock<std::mutex> lock(s->mu);
+    s->cv.notify_all();
+    s->cv_drain.wait(lock, [&] { return s->outstanding == 0; });
+    return s->failed ? SGEMM_B200_ERR_CUDA : SGEMM_B200_OK;
+}
+
+extern "C" int sgemm_b200_server_result(sgemm_b200_server* srv, int64_t id, double* latency_ms,
+                                        const float** C, int* ldc, int* batch_size) {
+    if (!srv) return SGEMM_B200_ERR_INVALID_ARG;
+    Server* s = &srv->s;
+    std::lock_guard<std::mutex> lock(s->mu);
+    auto it = s->all.find(id);
+    if (it == s->all.end()) return SGEMM_B200_ERR_INVALID_ARG;
+    Request* r = it->second;
+    if (r->state == sgb::serving::kRejected) return SGEMM_B200_ERR_REJECTED;
+    if (r->state != sgb::serving::kDone) return SGEMM_B200_ERR_CUDA;
+    if (latency_ms) *latency_ms = (r->t_done - r->t_submit) * 1e3;
+    if (C) *C = r->off >= 0 ? r->C : nullptr;
+    if (ldc) *ldc = r->n;
+    if (batch_size) *batch_size = r->batch_size;
+    return SGEMM_B200_OK;
+}
+
+extern "C" int sgemm_b200_server_read_result(sgemm_b200_server* srv, int64_t id, float* host_out) {
+    if (!srv || !host_out) return SGEMM_B200_ERR_INVALID_ARG;
+    Server* s = &srv->s;
+    const float* C = nullptr;
+    int m = 0, n = 0;
+    {
+        std::lock_guard<std::mutex> lock(s->mu);
+        auto it = s->all.find(id);
+        if (it == s->all.end()) return SGEMM_B200_ERR_INVALID_ARG;
+        Request* r = it->second;
+        if (r->state != sgb::serving::kDone || r->off < 0) return SGEMM_B200_ERR_INVALID_ARG;
+        C = r->C;
+        m = r->m;
+        n = r->n;
+    }
+    return sgb::cuda_status(
+        cudaMemcpy(host_out, C, sizeof(float) * (size_t)m * n, cudaMemcpyDeviceToHost));
+}
+
+extern "C" int sgemm_b200_server_release(sgemm_b200_server* srv, int64_t id) {
+    if (!srv) return SGEMM_B200_ERR_INVALID_ARG;
+    Server* s = &srv->s;
+    std::lock_guard<std::mutex> lock(s->mu);
+    auto it = s->all.find(id);
+    if (it == s->all.end()) return SGEMM_B200_ERR_INVALID_ARG;
+    Request* r = it->second;
+    if (r->state != sgb::serving::kDone && r->state != sgb::serving::kRejected &&
+        r->state != sgb::serving::kFailed)
+        return SGEMM_B200_ERR_INVALID_ARG;  // still queued or on the GPU
+    if (r->off >= 0) sgb::serving::pool_free(&s->pool, r->off);
+    delete r;
+    s->all.erase(it);
+    s->cv.notify_all();
+    return SGEMM_B200_OK;
+}
+
+extern "C" int sgemm_b200_server_get_stats(sgemm_b200_server* srv, sgemm_b200_server_stats* out) {
+    if (!srv || !out) return SGEMM_B200_ERR_INVALID_ARG;
+    Server* s = &srv->s;
+    std::lock_guard<std::mutex> lock(s->mu);
+    sgemm_b200_server_stats st{};
+    st.submitted = s->submitted;
+    st.completed = s->completed;
+    st.rejected = s->rejected;
+    st.failed = s->failed;
+    st.batches = s->batches;
+    st.max_batches_in_flight = s->max_in_flight;
+    st.max_batch_size = s->max_batch_seen;
+    std::vector<double> l = s->latencies_ms;
+    std::sort(l.begin(), l.end());
+    if (!l.empty()) {
+        auto pct = [&](double q) {
+            const size_t i = std::min(l.size() - 1, (size_t)std::ceil(q * l.size()) - 1);
+            return l[i];
+        };
+        st.p50_ms = pct(0.50);
+        st.p99_ms = pct(0.99);
+        double sum = 0;
+        for (double v : l) sum += v;
+        st.mean_ms = sum / l.size();
+        st.max_ms = l.back();
+    }
+    st.wall_s = s->t_first_submit >= 0 ? s->t_last_done - s->t_first_submit : 0;
+    st.gflops = st.wall_s > 0 ? s->flops_done / st.wall_s * 1e-9 : 0;
+    st.peak_pool_bytes = s->peak_pool;
+    st.peak_waiting = s->peak_waiting;
+    *out = st;
+    return SGEMM_B200_OK;
+}
+
+extern "C" int sgemm_b200_server_run_poisson(sgemm_b200_server* srv, double rate, int n,
+                                             uint64_t seed, sgemm_b200_server_stats* out) {
+    if (!srv || n < 0 || rate <= 0) return SGEMM_B200_ERR_INVALID_ARG;
+    Server* s = &srv->s;
+    std::vector<int> mnk(3 * (size_t)n);
+    std::vector<double> gaps(n);
+    sgb::serving::workload(n, rate, seed, mnk.data(), gaps.data());
+    {
+        // this run's statistics start fresh
+        std::lock_guard<std::mutex> lock(s->mu);
+        s->latencies_ms.clear();
+        s->flops_done = 0;
+        s->t_first_submit = -1;
+        s->t_last_done = 0;
+        s->submitted = s->completed = s->rejected = s->failed = s->batches = 0;
+        s->max_in_flight = s->max_batch_seen = 0;
+        s->peak_waiting = 0;
+    }
+    const int keep = s->cfg.keep_results;
+    s->cfg.keep_results = 0;  // an open-loop run releases results as they complete
+    auto t = sgb::serving::Clock::now();
+    std::vector<int64_t> ids;
+    for (int i = 0; i < n; ++i) {
+        t += std::chrono::duration_cast<sgb::serving::Clock::duration>(
+            std::chrono::duration<double>(gaps[i]));
+        std::this_thread::sleep_until(t);
+        int64_t id = 0;
+        sgemm_b200_server_submit(srv, mnk[3 * i], mnk[3 * i + 1], mnk[3 * i + 2], 1.0f, 0.0f,
+                                 seed * 1000003ull + i, &id);
+        ids.push_back(id);
+    }
+    const int d = sgemm_b200_server_drain(srv);
+    s->cfg.keep_results = keep;
+    for (int64_t id : ids) sgemm_b200_server_release(srv, id);
+    if (out) sgemm_b200_server_get_stats(srv, out);
+    return d;
+}
+
+extern "C" void sgemm_b200_server_destroy(sgemm_b200_server* srv) {
+    if (!srv) return;
+    Server* s = &srv->s;
+    {
+        std::lock_guard<std::mutex> lock(s->mu);
+        s->stop = true;
+        s->cv.notify_all();
+    }
+    if (s->worker.joinable()) s->worker.join();
+    cudaDeviceSynchronize();
+    for (auto& sl : s->slots) {
+        sgb::grouped::arena_release(&sl.arena);
+        if (sl.stream) cudaStreamDestroy(sl.stream);
+    }
+    if (s->ingest) cudaStreamDestroy(s->ingest);
+    for (auto& kv : s->all) {
+        if (kv.second->ready) cudaEventDestroy(kv.second->ready);
+        delete kv.second;
+    }
+    cudaFree(s->d_pool);
+    delete srv;
+}

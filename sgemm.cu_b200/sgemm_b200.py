@@ -55,6 +55,32 @@ class Problem(ctypes.Structure):
     ]
 
 
+class ServerConfig(ctypes.Structure):
+    """Mirror of sgemm_b200_server_config."""
+
+    _fields_ = [
+        ("hbm_budget_bytes", ctypes.c_size_t), ("slots", ctypes.c_int),
+        ("max_batch", ctypes.c_int), ("path", ctypes.c_int), ("keep_results", ctypes.c_int),
+        ("inject_alloc_failure_every", ctypes.c_int), ("inject_batch_delay_ms", ctypes.c_int),
+    ]
+
+
+class ServerStats(ctypes.Structure):
+    """Mirror of sgemm_b200_server_stats."""
+
+    _fields_ = [
+        ("submitted", ctypes.c_int64), ("completed", ctypes.c_int64),
+        ("rejected", ctypes.c_int64), ("failed", ctypes.c_int64), ("batches", ctypes.c_int64),
+        ("max_batches_in_flight", ctypes.c_int), ("max_batch_size", ctypes.c_int),
+        ("p50_ms", ctypes.c_double), ("p99_ms", ctypes.c_double), ("mean_ms", ctypes.c_double),
+        ("max_ms", ctypes.c_double), ("gflops", ctypes.c_double), ("wall_s", ctypes.c_double),
+        ("peak_pool_bytes", ctypes.c_size_t), ("peak_waiting", ctypes.c_int64),
+    ]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
 _lib: Optional[ctypes.CDLL] = None
 
 _I = ctypes.c_int
@@ -98,6 +124,27 @@ def _declare(lib: ctypes.CDLL) -> None:
     d("sgemm_b200_version", ctypes.c_char_p, [])
     d("sgemm", None, _GEMM_ARGS)
     d("sgemm_basic", None, _GEMM_ARGS)
+    S = ctypes.POINTER(ctypes.c_void_p)
+    d("sgemm_b200_server_create", _I, [S, ctypes.POINTER(ServerConfig)])
+    d("sgemm_b200_server_destroy", None, [_P])
+    d("sgemm_b200_server_submit", _I, [_P, _I, _I, _I, ctypes.c_float, ctypes.c_float,
+                                      ctypes.c_uint64, ctypes.POINTER(ctypes.c_int64)])
+    d("sgemm_b200_server_drain", _I, [_P])
+    d("sgemm_b200_server_result", _I, [_P, ctypes.c_int64, ctypes.POINTER(ctypes.c_double),
+                                      ctypes.POINTER(_P), ctypes.POINTER(_I), ctypes.POINTER(_I)])
+    d("sgemm_b200_server_read_result", _I, [_P, ctypes.c_int64, ctypes.c_void_p])
+    d("sgemm_b200_server_release", _I, [_P, ctypes.c_int64])
+    d("sgemm_b200_server_get_stats", _I, [_P, ctypes.POINTER(ServerStats)])
+    d("sgemm_b200_server_run_poisson", _I, [_P, ctypes.c_double, _I, ctypes.c_uint64,
+                                           ctypes.POINTER(ServerStats)])
+    d("sgemm_b200_serving_workload", _I, [_I, ctypes.c_double, ctypes.c_uint64,
+                                         ctypes.POINTER(_I), ctypes.POINTER(ctypes.c_double)])
+    d("sgemm_b200_pool_create", _P, [ctypes.c_size_t])
+    d("sgemm_b200_pool_destroy", None, [_P])
+    d("sgemm_b200_pool_alloc", ctypes.c_int64, [_P, ctypes.c_size_t])
+    d("sgemm_b200_pool_free", _I, [_P, ctypes.c_int64])
+    d("sgemm_b200_pool_used", ctypes.c_size_t, [_P])
+    d("sgemm_b200_pool_largest_free", ctypes.c_size_t, [_P])
 
 
 def lib() -> ctypes.CDLL:
@@ -303,3 +350,75 @@ class GroupedPlan:
             self.close()
         except Exception:
             pass
+
+
+# ------------------------------------------------------------------ serving --
+
+class Server:
+    """Continuous-batching GEMM server (include/sgemm_b200_serving.h)."""
+
+    def __init__(self, hbm_budget_bytes: int = 64 << 30, slots: int = 2, max_batch: int = 32,
+                 path="plain", keep_results: bool = False, inject_alloc_failure_every: int = 0,
+                 inject_batch_delay_ms: int = 0):
+        p = PATHS[path] if isinstance(path, str) else int(path)
+        self.cfg = ServerConfig(hbm_budget_bytes, slots, max_batch, p, 1 if keep_results else 0,
+                                inject_alloc_failure_every, inject_batch_delay_ms)
+        h = ctypes.c_void_p()
+        _check(lib().sgemm_b200_server_create(ctypes.byref(h), ctypes.byref(self.cfg)),
+               "server_create")
+        self._h = h
+
+    def submit(self, m: int, n: int, k: int, alpha: float = 1.0, beta: float = 0.0,
+               seed: int = 0) -> int:
+        rid = ctypes.c_int64()
+        _check(lib().sgemm_b200_server_submit(self._h, m, n, k, alpha, beta, seed,
+                                              ctypes.byref(rid)), "server_submit")
+        return rid.value
+
+    def drain(self) -> None:
+        _check(lib().sgemm_b200_server_drain(self._h), "server_drain")
+
+    def result(self, rid: int) -> dict:
+        lat, ptr, ld, bs = ctypes.c_double(), ctypes.c_void_p(), ctypes.c_int(), ctypes.c_int()
+        _check(lib().sgemm_b200_server_result(self._h, rid, ctypes.byref(lat), ctypes.byref(ptr),
+                                              ctypes.byref(ld), ctypes.byref(bs)), "result")
+        return {"latency_ms": lat.value, "C": ptr.value, "ldc": ld.value, "batch_size": bs.value}
+
+    def read_result(self, rid: int, m: int, n: int):
+        import numpy as np
+        out = np.empty((m, n), dtype=np.float32)
+        _check(lib().sgemm_b200_server_read_result(self._h, rid, out.ctypes.data), "read_result")
+        return out
+
+    def release(self, rid: int) -> None:
+        _check(lib().sgemm_b200_server_release(self._h, rid), "release")
+
+    def stats(self) -> dict:
+        st = ServerStats()
+        _check(lib().sgemm_b200_server_get_stats(self._h, ctypes.byref(st)), "stats")
+        return st.as_dict()
+
+    def run_poisson(self, rate_per_s: float, n_requests: int, seed: int = 0) -> dict:
+        st = ServerStats()
+        _check(lib().sgemm_b200_server_run_poisson(self._h, rate_per_s, n_requests, seed,
+                                                   ctypes.byref(st)), "run_poisson")
+        return st.as_dict()
+
+    def close(self) -> None:
+        if self._h:
+            lib().sgemm_b200_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def serving_workload(n: int, rate: float, seed: int):
+    """The serving mix (host-only): list of (m, n, k) and inter-arrival gaps."""
+    mnk = (ctypes.c_int * (3 * n))()
+    gaps = (ctypes.c_double * n)()
+    _check(lib().sgemm_b200_serving_workload(n, rate, seed, mnk, gaps), "serving_workload")
+    return [tuple(mnk[3 * i:3 * i + 3]) for i in range(n)], list(gaps)
