@@ -116,12 +116,19 @@ def _init_dist(world: int, local: int):
 
 
 def _max_over_ranks(dist, value: float) -> float:
+    """Max of a per-rank value (device time) over all ranks."""
     if dist is None:
         return value
     import torch
-    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([value], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def _job_gflops(flop_per_step: float, world: int, steps: int, max_total_ms: float) -> float:
+    """Whole-job throughput: every rank's steps over the slowest rank's time."""
+    return flop_per_step * world * steps / (max_total_ms * 1e-3) * 1e-9
 
 
 def _barrier(dist):
@@ -386,20 +393,17 @@ def _serving_leg(sg, rates, n_requests):
 # --------------------------------------------------------------------- main --
 
 def run(args):
-    import torch
     rank, world, local = _dist_env()
+    if args.impl == "reference" and rank != 0:
+        return  # the reference arm runs on rank 0 only; other ranks exit without work
+    import torch
     torch.cuda.set_device(local)
-    dist = _init_dist(world, local)
     peaks, peak_src = _peaks()
     props = torch.cuda.get_device_properties(local)
     sms = props.multi_processor_count
-
     if args.impl == "reference":
-        if rank != 0:
-            if dist is not None:
-                dist.destroy_process_group()
-            return
         return run_reference(args, torch, peaks, sms, local)
+    dist = _init_dist(world, local)
 
     import sgemm_b200 as sg
     A, B, C = _alloc_inputs(torch, sg, SIZE)
@@ -430,7 +434,7 @@ def run(args):
     total_ms = _max_over_ranks(dist, sum(ms))
     ms_step = total_ms / args.steps
     flops = 2.0 * SIZE ** 3
-    value = flops * world * args.steps / (total_ms * 1e-3) * 1e-9  # GFLOP/s, whole job
+    value = _job_gflops(flops, world, args.steps, total_ms)  # GFLOP/s, whole job
 
     # roofline: FP32 SIMT peak (SMs x 128 FMA/clk x 2) at max and observed clock
     sm_max = clk.get("sm_max_mhz") or peaks.get("sm_max_mhz", 1965.0)

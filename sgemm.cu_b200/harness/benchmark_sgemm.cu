@@ -12,6 +12,12 @@
 // per-iteration times on stdout, --path (plain|bf16x6|tf32x3), --alpha/--beta,
 // --dist, and the L2 flush buffer is allocated once (the reference mallocs it
 // on every iteration, common/helper_cuda.h:70-83).
+//
+// --lib=cublas times cublasSgemm instead (the reference's -DCUBLAS=1 lane,
+// benchmark.cu:150-164): row-major C = A*B issued as the column-major
+// C^T = B^T * A^T, default math mode (no TF32).
+#include <cublas_v2.h>
+
 #include <algorithm>
 #include <filesystem>
 #include <fstream>
@@ -31,6 +37,23 @@ int main(int argc, char** argv) {
     const int dist = parse_dist(flag_str(argc, argv, "dist", "u01"));
     const float alpha = (float)flag_double(argc, argv, "alpha", 1.0);
     const float beta = (float)flag_double(argc, argv, "beta", 0.0);
+    const bool use_cublas = flag_str(argc, argv, "lib", "sgemm_b200") == "cublas";
+    cublasHandle_t handle = nullptr;
+    if (use_cublas && cublasCreate(&handle) != CUBLAS_STATUS_SUCCESS) {
+        std::fprintf(stderr, "cublasCreate failed\n");
+        return 2;
+    }
+    auto gemm = [&](int s, float* A, float* B, float* C) {
+        if (use_cublas) {
+            if (cublasSgemm(handle, CUBLAS_OP_N, CUBLAS_OP_N, s, s, s, &alpha, B, s, A, s, &beta,
+                            C, s) != CUBLAS_STATUS_SUCCESS) {
+                std::fprintf(stderr, "cublasSgemm failed\n");
+                std::exit(2);
+            }
+        } else {
+            SCHECK(sgemm_b200_gemm(path, s, s, s, &alpha, A, s, B, s, &beta, C, s, nullptr));
+        }
+    };
 
     int dev = 0, l2 = 0;
     HCHECK(cudaGetDevice(&dev));
@@ -50,7 +73,7 @@ int main(int argc, char** argv) {
         SCHECK(sgemm_b200_fill_random(B, s, s, s, 7, 2, dist, nullptr));
         SCHECK(sgemm_b200_fill_random(C, s, s, s, 7, 3, dist, nullptr));
         for (int i = 0; i < wniter; ++i) {
-            SCHECK(sgemm_b200_gemm(path, s, s, s, &alpha, A, s, B, s, &beta, C, s, nullptr));
+            gemm(s, A, B, C);
             HCHECK(cudaDeviceSynchronize());
         }
         HCHECK(cudaFree(A));
@@ -76,7 +99,7 @@ int main(int argc, char** argv) {
         HCHECK(cudaEventCreate(&e1));
         for (int j = 0; j < n_iter; ++j) {
             HCHECK(cudaEventRecord(e0));
-            SCHECK(sgemm_b200_gemm(path, s, s, s, &alpha, A, s, B, s, &beta, C, s, nullptr));
+            gemm(s, A, B, C);
             HCHECK(cudaEventRecord(e1));
             HCHECK(cudaEventSynchronize(e1));
             HCHECK(cudaEventElapsedTime(&ms[j], e0, e1));
@@ -107,5 +130,6 @@ int main(int argc, char** argv) {
     for (size_t i = 0; i < sizes.size(); ++i) f << sizes[i] << " " << gflops[i] << "\n";
     std::printf("Benchmark data stored in %s\n", out.c_str());
     HCHECK(cudaFree(flush));
+    if (handle) cublasDestroy(handle);
     return 0;
 }
