@@ -18,11 +18,17 @@ using C1 = Cfg<128, 128, 4, 2, 8, 3, kLoaderTma, 2>;      // 8 warps,  96 KB, 2/
 using C2 = Cfg<128, 128, 4, 1, 16, 3, kLoaderTma, 2>;     // 4 warps,  96 KB, 2/SM
 using C3 = Cfg<64, 128, 2, 2, 8, 4, kLoaderTma, 2>;       // 4 warps,  96 KB, 2/SM
 using C4 = Cfg<64, 64, 2, 1, 8, 4, kLoaderTma, 3>;        // 2 warps,  64 KB, 3/SM
-using C5 = Cfg<128, 256, 4, 2, 16, 4, kLoaderAsync4, 1>;
-using C6 = Cfg<128, 128, 4, 2, 8, 3, kLoaderAsync4, 2>;
-using C7 = Cfg<128, 128, 4, 1, 16, 3, kLoaderAsync4, 2>;
-using C8 = Cfg<64, 128, 2, 2, 8, 4, kLoaderAsync4, 2>;
-using C9 = Cfg<64, 64, 2, 1, 8, 4, kLoaderAsync4, 3>;
+using C5 = Cfg<64, 128, 2, 2, 8, 3, kLoaderTma, 3>;       // 4 warps,  72 KB, 3/SM
+using C6 = Cfg<128, 64, 4, 1, 8, 3, kLoaderTma, 3>;       // 4 warps,  72 KB, 3/SM
+using C7 = Cfg<64, 128, 2, 2, 8, 4, kLoaderTma, 2, 2>;    // C3 with the k loop unrolled 2x
+using C8 = Cfg<128, 256, 4, 2, 16, 4, kLoaderAsync4, 1>;
+using C9 = Cfg<128, 128, 4, 2, 8, 3, kLoaderAsync4, 2>;
+using C10 = Cfg<128, 128, 4, 1, 16, 3, kLoaderAsync4, 2>;
+using C11 = Cfg<64, 128, 2, 2, 8, 4, kLoaderAsync4, 2>;
+using C12 = Cfg<64, 64, 2, 1, 8, 4, kLoaderAsync4, 3>;
+using C13 = Cfg<64, 128, 2, 2, 8, 3, kLoaderAsync4, 3>;
+using C14 = Cfg<128, 64, 4, 1, 8, 3, kLoaderAsync4, 3>;
+using C15 = Cfg<64, 128, 2, 2, 8, 4, kLoaderAsync4, 2, 2>;
 
 struct ConfigDesc {
     const char* name;
@@ -40,11 +46,14 @@ constexpr ConfigDesc describe(const char* name, float eff) {
 // Efficiencies: GFLOP/s measured on a B200 at 8192^3 (alpha=1.5, beta=0.5),
 // normalised to the best configuration of the same loader.
 static const ConfigDesc kConfigs[] = {
-    describe<C0>("tma_128x256_w8_t8x16_s4", 0.956f), describe<C1>("tma_128x128_w8_t8x8_s3", 0.99f),
-    describe<C2>("tma_128x128_w4_t8x16_s3", 0.95f),  describe<C3>("tma_64x128_w4_t8x8_s4", 1.00f),
-    describe<C4>("tma_64x64_w2_t8x8_s4", 0.88f),     describe<C5>("cpa_128x256_w8_t8x16_s4", 0.75f),
-    describe<C6>("cpa_128x128_w8_t8x8_s3", 0.71f),   describe<C7>("cpa_128x128_w4_t8x16_s3", 0.72f),
-    describe<C8>("cpa_64x128_w4_t8x8_s4", 0.64f),    describe<C9>("cpa_64x64_w2_t8x8_s4", 0.50f),
+    describe<C0>("tma_128x256_w8_t8x16_s4", 0.956f),  describe<C1>("tma_128x128_w8_t8x8_s3", 0.99f),
+    describe<C2>("tma_128x128_w4_t8x16_s3", 0.95f),   describe<C3>("tma_64x128_w4_t8x8_s4", 1.00f),
+    describe<C4>("tma_64x64_w2_t8x8_s4", 0.88f),      describe<C5>("tma_64x128_w4_t8x8_s3", 0.98f),
+    describe<C6>("tma_128x64_w4_t8x8_s3", 0.97f),     describe<C7>("tma_64x128_w4_t8x8_s4_u2", 0.97f),
+    describe<C8>("cpa_128x256_w8_t8x16_s4", 0.75f),   describe<C9>("cpa_128x128_w8_t8x8_s3", 0.71f),
+    describe<C10>("cpa_128x128_w4_t8x16_s3", 0.72f),  describe<C11>("cpa_64x128_w4_t8x8_s4", 0.64f),
+    describe<C12>("cpa_64x64_w2_t8x8_s4", 0.50f),     describe<C13>("cpa_64x128_w4_t8x8_s3", 0.62f),
+    describe<C14>("cpa_128x64_w4_t8x8_s3", 0.62f),    describe<C15>("cpa_64x128_w4_t8x8_s4_u2", 0.62f),
 };
 constexpr int kNumConfigs = sizeof(kConfigs) / sizeof(kConfigs[0]);
 constexpr int kNumPerLoader = kNumConfigs / 2;

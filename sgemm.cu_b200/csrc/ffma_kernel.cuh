@@ -34,11 +34,13 @@ namespace ffma {
 
 enum Loader { kLoaderTma = 0, kLoaderAsync4 = 1 };
 
-template <int BM_, int BN_, int WM_, int WN_, int TN_, int STAGES_, int LOADER_, int MINB_ = 1>
+template <int BM_, int BN_, int WM_, int WN_, int TN_, int STAGES_, int LOADER_, int MINB_ = 1,
+          int K4U_ = 8>
 struct Cfg {
     static constexpr int BM = BM_, BN = BN_, WM = WM_, WN = WN_, TN = TN_, STAGES = STAGES_;
     static constexpr int LOADER = LOADER_;
     static constexpr int MINB = MINB_;  // resident CTAs per SM the register budget targets
+    static constexpr int K4U = K4U_;    // unroll of the 8 four-deep k steps of a k block
     static constexpr int BK = 32;  // one 128-byte row of A per k block
     static constexpr int TM = 8;
     static constexpr int THREADS = 32 * WM * WN;
@@ -72,7 +74,7 @@ __device__ __forceinline__ void compute_stage(const uint8_t* __restrict__ As,
                                               const uint8_t* __restrict__ Bs, uint32_t a_base,
                                               uint32_t xa0, uint32_t xa1, uint32_t b_base,
                                               float (&acc)[C::TM][C::TN]) {
-#pragma unroll
+#pragma unroll C::K4U
     for (int k4 = 0; k4 < C::BK / 4; ++k4) {
         float4 a[C::TM];
 #pragma unroll

@@ -502,6 +502,32 @@ static int launch(int m, int n, int k, float alpha, const float* A, int lda, con
 
 }  // namespace split
 
+// Library-owned stream-ordered memory pool for NULL-workspace calls, one per
+// device.  Its release threshold is unlimited, so freed workspaces stay in the
+// pool and the next call reuses them instead of going back to the driver; the
+// caller's default pool is left untouched.
+static cudaMemPool_t workspace_pool() {
+    static cudaMemPool_t pools[64] = {nullptr};
+    static std::mutex mu;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+    std::lock_guard<std::mutex> lock(mu);
+    if (!pools[dev]) {
+        cudaMemPoolProps props;
+        std::memset(&props, 0, sizeof(props));
+        props.allocType = cudaMemAllocationTypePinned;
+        props.handleTypes = cudaMemHandleTypeNone;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        cudaMemPool_t p = nullptr;
+        if (cudaMemPoolCreate(&p, &props) != cudaSuccess) return nullptr;
+        uint64_t threshold = ~0ull;
+        cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &threshold);
+        pools[dev] = p;
+    }
+    return pools[dev];
+}
+
 int split_launch(int path, int m, int n, int k, float alpha, const float* A, int lda,
                  const float* B, int ldb, float beta, float* C, int ldc, void* ws,
                  size_t ws_bytes, cudaStream_t stream) {
@@ -514,7 +540,9 @@ int split_launch(int path, int m, int n, int k, float alpha, const float* A, int
                             : split::workspace_bytes<SGEMM_B200_PATH_TF32X3>(m, n, k);
     bool owned = false;
     if (!ws) {
-        cudaError_t e = cudaMallocAsync(&ws, need, stream);
+        cudaMemPool_t pool = workspace_pool();
+        if (!pool) return SGEMM_B200_ERR_CUDA;
+        cudaError_t e = cudaMallocFromPoolAsync(&ws, need, pool, stream);
         if (e != cudaSuccess) return cuda_status(e);
         ws_bytes = need;
         owned = true;
