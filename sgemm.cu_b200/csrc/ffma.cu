@@ -21,6 +21,12 @@ using C4 = Cfg<64, 64, 2, 1, 8, 4, kLoaderTma, 3>;        // 2 warps,  64 KB, 3/
 using C5 = Cfg<64, 128, 2, 2, 8, 3, kLoaderTma, 3>;       // 4 warps,  72 KB, 3/SM
 using C6 = Cfg<128, 64, 4, 1, 8, 3, kLoaderTma, 3>;       // 4 warps,  72 KB, 3/SM
 using C7 = Cfg<64, 128, 2, 2, 8, 4, kLoaderTma, 2, 2>;    // C3 with the k loop unrolled 2x
+using C7p = Cfg<64, 128, 2, 2, 8, 4, kLoaderTma, 2, 8, 1>;  // C3, pipelined fragments
+using C7q = Cfg<128, 128, 4, 2, 8, 3, kLoaderTma, 1, 8, 1>; // 8 warps, pipelined, 1/SM regs
+using W0 = Cfg<128, 256, 4, 2, 16, 4, kLoaderTma, 1, 8, 1>;  // 8x16 thread tile, LDS.128 pipe
+using W1 = Cfg<128, 256, 4, 2, 16, 4, kLoaderTma, 1, 8, 2>;  // 8x16, A via LDS.64 pipe
+using W2 = Cfg<128, 128, 4, 1, 16, 3, kLoaderTma, 2, 8, 1>;  // 4 warps x 2 CTAs/SM
+using W3 = Cfg<128, 128, 4, 1, 16, 3, kLoaderTma, 2, 8, 2>;
 using C8 = Cfg<128, 256, 4, 2, 16, 4, kLoaderAsync4, 1>;
 using C9 = Cfg<128, 128, 4, 2, 8, 3, kLoaderAsync4, 2>;
 using C10 = Cfg<128, 128, 4, 1, 16, 3, kLoaderAsync4, 2>;
@@ -29,6 +35,8 @@ using C12 = Cfg<64, 64, 2, 1, 8, 4, kLoaderAsync4, 3>;
 using C13 = Cfg<64, 128, 2, 2, 8, 3, kLoaderAsync4, 3>;
 using C14 = Cfg<128, 64, 4, 1, 8, 3, kLoaderAsync4, 3>;
 using C15 = Cfg<64, 128, 2, 2, 8, 4, kLoaderAsync4, 2, 2>;
+using C15p = Cfg<64, 128, 2, 2, 8, 4, kLoaderAsync4, 2, 8, 1>;
+using C15q = Cfg<128, 128, 4, 2, 8, 3, kLoaderAsync4, 1, 8, 1>;
 
 struct ConfigDesc {
     const char* name;
@@ -50,13 +58,16 @@ static const ConfigDesc kConfigs[] = {
     describe<C2>("tma_128x128_w4_t8x16_s3", 0.95f),   describe<C3>("tma_64x128_w4_t8x8_s4", 1.00f),
     describe<C4>("tma_64x64_w2_t8x8_s4", 0.88f),      describe<C5>("tma_64x128_w4_t8x8_s3", 0.98f),
     describe<C6>("tma_128x64_w4_t8x8_s3", 0.97f),     describe<C7>("tma_64x128_w4_t8x8_s4_u2", 0.97f),
+    describe<C7p>("tma_64x128_w4_t8x8_s4_pipe", 0.97f), describe<C7q>("tma_128x128_w8_t8x8_s3_pipe", 0.97f),
+    describe<W0>("tma_128x256_w8_t8x16_s4_pipe", 0.95f), describe<W1>("tma_128x256_w8_t8x16_s4_p64", 0.95f),
+    describe<W2>("tma_128x128_w4_t8x16_s3_pipe", 0.95f), describe<W3>("tma_128x128_w4_t8x16_s3_p64", 0.95f),
     describe<C8>("cpa_128x256_w8_t8x16_s4", 0.75f),   describe<C9>("cpa_128x128_w8_t8x8_s3", 0.71f),
     describe<C10>("cpa_128x128_w4_t8x16_s3", 0.72f),  describe<C11>("cpa_64x128_w4_t8x8_s4", 0.64f),
     describe<C12>("cpa_64x64_w2_t8x8_s4", 0.50f),     describe<C13>("cpa_64x128_w4_t8x8_s3", 0.62f),
     describe<C14>("cpa_128x64_w4_t8x8_s3", 0.62f),    describe<C15>("cpa_64x128_w4_t8x8_s4_u2", 0.62f),
+    describe<C15p>("cpa_64x128_w4_t8x8_s4_pipe", 0.62f), describe<C15q>("cpa_128x128_w8_t8x8_s3_pipe", 0.62f),
 };
 constexpr int kNumConfigs = sizeof(kConfigs) / sizeof(kConfigs[0]);
-constexpr int kNumPerLoader = kNumConfigs / 2;
 
 static int occupancy(int cfg) {
     static int occ[64][kNumConfigs];
@@ -103,18 +114,19 @@ int plain_config_tile(int cfg, int* bm, int* bn) {
 // CTAs of one wave share an SM, so each takes `resident` times as long.
 int plain_select(int m, int n, int k, const float* A, int lda, const float* B, int ldb) {
     using namespace ffma;
-    const int base = (k == 0 || tma_ok(A, lda, B, ldb)) ? 0 : kNumPerLoader;
+    const int loader = (k == 0 || tma_ok(A, lda, B, ldb)) ? kLoaderTma : kLoaderAsync4;
     const DeviceInfo& d = device_info();
     const int sms = d.sm_count > 0 ? d.sm_count : 148;
-    int best = base;
+    int best = -1;
     double best_t = 1e300;
-    for (int c = base; c < base + kNumPerLoader; ++c) {
+    for (int c = 0; c < kNumConfigs; ++c) {
         const ConfigDesc& cd = kConfigs[c];
+        if (cd.loader != loader) continue;
         const double tiles = double(div_up(m, cd.bm)) * div_up(n, cd.bn);
         const double slots = double(sms) * occupancy(c);
         const double waves = std::ceil(tiles / slots);
         const double t = waves * double(cd.bm) * cd.bn * occupancy(c) / cd.efficiency;
-        if (t < best_t * 0.999) {
+        if (best < 0 || t < best_t * 0.999) {
             best_t = t;
             best = c;
         }

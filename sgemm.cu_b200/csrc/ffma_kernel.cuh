@@ -35,12 +35,13 @@ namespace ffma {
 enum Loader { kLoaderTma = 0, kLoaderAsync4 = 1 };
 
 template <int BM_, int BN_, int WM_, int WN_, int TN_, int STAGES_, int LOADER_, int MINB_ = 1,
-          int K4U_ = 8>
+          int K4U_ = 8, int PIPE_ = 0>
 struct Cfg {
     static constexpr int BM = BM_, BN = BN_, WM = WM_, WN = WN_, TN = TN_, STAGES = STAGES_;
     static constexpr int LOADER = LOADER_;
     static constexpr int MINB = MINB_;  // resident CTAs per SM the register budget targets
     static constexpr int K4U = K4U_;    // unroll of the 8 four-deep k steps of a k block
+    static constexpr int PIPE = PIPE_;  // 1: double-buffered LDS.128 fragments, 2: A via LDS.64
     static constexpr int BK = 32;  // one 128-byte row of A per k block
     static constexpr int TM = 8;
     static constexpr int THREADS = 32 * WM * WN;
@@ -68,12 +69,125 @@ __device__ __forceinline__ void tile_coords(int bid, int tiles_m, int tiles_n, i
     tn = r / gsz;
 }
 
+// Fragment loads of one k block: A rows for the 4-deep step k4 (4 k-values of
+// each of the thread's 8 rows) and B columns for one k.
+template <class C>
+__device__ __forceinline__ void load_a_frag(const uint8_t* __restrict__ As, uint32_t a_base,
+                                            uint32_t xa0, uint32_t xa1, int k4,
+                                            float4 (&a)[C::TM]) {
+#pragma unroll
+    for (int i = 0; i < C::TM; ++i) {
+        const uint32_t x = (i & 1) ? xa1 : xa0;
+        const uint32_t off = a_base + i * 4 * 128 + ((static_cast<uint32_t>(k4) << 4) ^ x);
+        a[i] = *reinterpret_cast<const float4*>(As + off);
+    }
+}
+
+template <class C>
+__device__ __forceinline__ void load_b_frag(const uint8_t* __restrict__ Bs, uint32_t b_base, int k,
+                                            float4 (&b)[C::TN / 4]) {
+#pragma unroll
+    for (int g = 0; g < C::TN / 4; ++g)
+        b[g] = *reinterpret_cast<const float4*>(Bs + k * C::BN * 4 + b_base + g * 128);
+}
+
+// Same arithmetic as compute_stage, with the next fragments loaded one step
+// ahead into a second register set (A one 4-deep step ahead, B one k ahead),
+// so shared-memory latency overlaps the current step's FFMAs.
+template <class C>
+__device__ __forceinline__ void compute_stage_pipelined(const uint8_t* __restrict__ As,
+                                                        const uint8_t* __restrict__ Bs,
+                                                        uint32_t a_base, uint32_t xa0,
+                                                        uint32_t xa1, uint32_t b_base,
+                                                        float (&acc)[C::TM][C::TN]) {
+    float4 a[2][C::TM];
+    float4 b[2][C::TN / 4];
+    load_a_frag<C>(As, a_base, xa0, xa1, 0, a[0]);
+    load_b_frag<C>(Bs, b_base, 0, b[0]);
+#pragma unroll
+    for (int k4 = 0; k4 < C::BK / 4; ++k4) {
+#pragma unroll
+        for (int kk = 0; kk < 4; ++kk) {
+            const int k = 4 * k4 + kk;
+            if (kk == 0 && k4 + 1 < C::BK / 4)
+                load_a_frag<C>(As, a_base, xa0, xa1, k4 + 1, a[(k4 + 1) & 1]);
+            if (k + 1 < C::BK) load_b_frag<C>(Bs, b_base, k + 1, b[(k + 1) & 1]);
+            const float4(&ac)[C::TM] = a[k4 & 1];
+            const float4(&bc)[C::TN / 4] = b[k & 1];
+#pragma unroll
+            for (int i = 0; i < C::TM; ++i) {
+                const float av = kk == 0 ? ac[i].x : kk == 1 ? ac[i].y : kk == 2 ? ac[i].z : ac[i].w;
+#pragma unroll
+                for (int g = 0; g < C::TN / 4; ++g) {
+                    acc[i][4 * g + 0] = fmaf(av, bc[g].x, acc[i][4 * g + 0]);
+                    acc[i][4 * g + 1] = fmaf(av, bc[g].y, acc[i][4 * g + 1]);
+                    acc[i][4 * g + 2] = fmaf(av, bc[g].z, acc[i][4 * g + 2]);
+                    acc[i][4 * g + 3] = fmaf(av, bc[g].w, acc[i][4 * g + 3]);
+                }
+            }
+        }
+    }
+}
+
+// Variant for wide thread tiles (8 x 16): A is read two k-values at a time
+// (LDS.64), halving the registers its double buffer needs; B one k ahead.
+template <class C>
+__device__ __forceinline__ void compute_stage_pipelined64(const uint8_t* __restrict__ As,
+                                                          const uint8_t* __restrict__ Bs,
+                                                          uint32_t a_base, uint32_t xa0,
+                                                          uint32_t xa1, uint32_t b_base,
+                                                          float (&acc)[C::TM][C::TN]) {
+    float2 a[2][C::TM];
+    float4 b[2][C::TN / 4];
+    auto load_a2 = [&](int kp, float2 (&dst)[C::TM]) {
+#pragma unroll
+        for (int i = 0; i < C::TM; ++i) {
+            const uint32_t x = (i & 1) ? xa1 : xa0;
+            const uint32_t off = a_base + i * 4 * 128 +
+                                 ((static_cast<uint32_t>(kp >> 1) << 4) ^ x) + ((kp & 1) << 3);
+            dst[i] = *reinterpret_cast<const float2*>(As + off);
+        }
+    };
+    load_a2(0, a[0]);
+    load_b_frag<C>(Bs, b_base, 0, b[0]);
+#pragma unroll
+    for (int kp = 0; kp < C::BK / 2; ++kp) {
+#pragma unroll
+        for (int kk = 0; kk < 2; ++kk) {
+            const int k = 2 * kp + kk;
+            if (kk == 0 && kp + 1 < C::BK / 2) load_a2(kp + 1, a[(kp + 1) & 1]);
+            if (k + 1 < C::BK) load_b_frag<C>(Bs, b_base, k + 1, b[(k + 1) & 1]);
+            const float2(&ac)[C::TM] = a[kp & 1];
+            const float4(&bc)[C::TN / 4] = b[k & 1];
+#pragma unroll
+            for (int i = 0; i < C::TM; ++i) {
+                const float av = kk == 0 ? ac[i].x : ac[i].y;
+#pragma unroll
+                for (int g = 0; g < C::TN / 4; ++g) {
+                    acc[i][4 * g + 0] = fmaf(av, bc[g].x, acc[i][4 * g + 0]);
+                    acc[i][4 * g + 1] = fmaf(av, bc[g].y, acc[i][4 * g + 1]);
+                    acc[i][4 * g + 2] = fmaf(av, bc[g].z, acc[i][4 * g + 2]);
+                    acc[i][4 * g + 3] = fmaf(av, bc[g].w, acc[i][4 * g + 3]);
+                }
+            }
+        }
+    }
+}
+
 // Accumulate one 32-deep k block held in shared memory.
 template <class C>
 __device__ __forceinline__ void compute_stage(const uint8_t* __restrict__ As,
                                               const uint8_t* __restrict__ Bs, uint32_t a_base,
                                               uint32_t xa0, uint32_t xa1, uint32_t b_base,
                                               float (&acc)[C::TM][C::TN]) {
+    if constexpr (C::PIPE == 1) {
+        compute_stage_pipelined<C>(As, Bs, a_base, xa0, xa1, b_base, acc);
+        return;
+    }
+    if constexpr (C::PIPE == 2) {
+        compute_stage_pipelined64<C>(As, Bs, a_base, xa0, xa1, b_base, acc);
+        return;
+    }
 #pragma unroll C::K4U
     for (int k4 = 0; k4 < C::BK / 4; ++k4) {
         float4 a[C::TM];
