@@ -174,20 +174,13 @@ __device__ __forceinline__ void compute_stage_pipelined64(const uint8_t* __restr
     }
 }
 
-// Accumulate one 32-deep k block held in shared memory.
+// Fragment-at-a-time core: A for a 4-deep step at its start, B per k (the
+// compiler schedules the loads).
 template <class C>
-__device__ __forceinline__ void compute_stage(const uint8_t* __restrict__ As,
-                                              const uint8_t* __restrict__ Bs, uint32_t a_base,
-                                              uint32_t xa0, uint32_t xa1, uint32_t b_base,
-                                              float (&acc)[C::TM][C::TN]) {
-    if constexpr (C::PIPE == 1) {
-        compute_stage_pipelined<C>(As, Bs, a_base, xa0, xa1, b_base, acc);
-        return;
-    }
-    if constexpr (C::PIPE == 2) {
-        compute_stage_pipelined64<C>(As, Bs, a_base, xa0, xa1, b_base, acc);
-        return;
-    }
+__device__ __forceinline__ void compute_stage_simple(const uint8_t* __restrict__ As,
+                                                     const uint8_t* __restrict__ Bs,
+                                                     uint32_t a_base, uint32_t xa0, uint32_t xa1,
+                                                     uint32_t b_base, float (&acc)[C::TM][C::TN]) {
 #pragma unroll C::K4U
     for (int k4 = 0; k4 < C::BK / 4; ++k4) {
         float4 a[C::TM];
@@ -217,6 +210,21 @@ __device__ __forceinline__ void compute_stage(const uint8_t* __restrict__ As,
             }
         }
     }
+}
+
+// Accumulate one 32-deep k block held in shared memory.  Every variant
+// accumulates each element over k in increasing order with one FMA per term.
+template <class C>
+__device__ __forceinline__ void compute_stage(const uint8_t* __restrict__ As,
+                                              const uint8_t* __restrict__ Bs, uint32_t a_base,
+                                              uint32_t xa0, uint32_t xa1, uint32_t b_base,
+                                              float (&acc)[C::TM][C::TN]) {
+    if constexpr (C::PIPE == 1)
+        compute_stage_pipelined<C>(As, Bs, a_base, xa0, xa1, b_base, acc);
+    else if constexpr (C::PIPE == 2)
+        compute_stage_pipelined64<C>(As, Bs, a_base, xa0, xa1, b_base, acc);
+    else
+        compute_stage_simple<C>(As, Bs, a_base, xa0, xa1, b_base, acc);
 }
 
 // Operand and output views of one GEMM, shared by the single-problem kernel
