@@ -107,6 +107,28 @@ bool encode_tensor_map_3d(CUtensorMap* map, CUtensorMapDataType dtype, const voi
     return r == CUDA_SUCCESS;
 }
 
+cudaMemPool_t library_pool() {
+    static cudaMemPool_t pools[kMaxDevices] = {nullptr};
+    static std::mutex mu;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return nullptr;
+    std::lock_guard<std::mutex> lock(mu);
+    if (!pools[dev]) {
+        cudaMemPoolProps props;
+        std::memset(&props, 0, sizeof(props));
+        props.allocType = cudaMemAllocationTypePinned;
+        props.handleTypes = cudaMemHandleTypeNone;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        cudaMemPool_t p = nullptr;
+        if (cudaMemPoolCreate(&p, &props) != cudaSuccess) return nullptr;
+        uint64_t threshold = ~0ull;
+        cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &threshold);
+        pools[dev] = p;
+    }
+    return pools[dev];
+}
+
 int check_gemm_args(int m, int n, int k, const float* alpha, const void* A, int lda,
                     const void* B, int ldb, const float* beta, const void* C, int ldc) {
     if (m < 0 || n < 0 || k < 0) return SGEMM_B200_ERR_INVALID_ARG;

@@ -51,6 +51,13 @@ bool encode_tensor_map_3d(CUtensorMap* map, CUtensorMapDataType dtype, const voi
                           uint64_t outer_stride_bytes, uint32_t box_inner, uint32_t box_mid,
                           uint32_t box_outer, CUtensorMapSwizzle swizzle);
 
+// Library-owned stream-ordered memory pool of the current device, for
+// scratch the library allocates itself (split-path workspaces when the caller
+// passes none, packed copies of unaligned operands).  Its release threshold is
+// unlimited, so freed blocks are reused by the next call instead of going back
+// to the driver; the caller's default pool is left untouched.
+cudaMemPool_t library_pool();
+
 // Shape checks common to every entry point.  Returns SGEMM_B200_OK or
 // SGEMM_B200_ERR_INVALID_ARG.
 int check_gemm_args(int m, int n, int k, const float* alpha, const void* A, int lda,

@@ -13,30 +13,25 @@ namespace ffma {
 
 // Compiled configurations.  Index = public config id.
 //   tile      warps  thread tile  stages  loader   resident CTAs/SM
-using C0 = Cfg<128, 256, 4, 2, 16, 4, kLoaderTma, 1>;     // 8 warps, 192 KB smem, 1/SM
-using C1 = Cfg<128, 128, 4, 2, 8, 3, kLoaderTma, 2>;      // 8 warps,  96 KB, 2/SM
-using C2 = Cfg<128, 128, 4, 1, 16, 3, kLoaderTma, 2>;     // 4 warps,  96 KB, 2/SM
-using C3 = Cfg<64, 128, 2, 2, 8, 4, kLoaderTma, 2>;       // 4 warps,  96 KB, 2/SM
-using C4 = Cfg<64, 64, 2, 1, 8, 4, kLoaderTma, 3>;        // 2 warps,  64 KB, 3/SM
-using C5 = Cfg<64, 128, 2, 2, 8, 3, kLoaderTma, 3>;       // 4 warps,  72 KB, 3/SM
-using C6 = Cfg<128, 64, 4, 1, 8, 3, kLoaderTma, 3>;       // 4 warps,  72 KB, 3/SM
-using C7 = Cfg<64, 128, 2, 2, 8, 4, kLoaderTma, 2, 2>;    // C3 with the k loop unrolled 2x
-using C7p = Cfg<64, 128, 2, 2, 8, 4, kLoaderTma, 2, 8, 1>;  // C3, pipelined fragments
-using C7q = Cfg<128, 128, 4, 2, 8, 3, kLoaderTma, 1, 8, 1>; // 8 warps, pipelined, 1/SM regs
-using W0 = Cfg<128, 256, 4, 2, 16, 4, kLoaderTma, 1, 8, 1>;  // 8x16 thread tile, LDS.128 pipe
-using W1 = Cfg<128, 256, 4, 2, 16, 4, kLoaderTma, 1, 8, 2>;  // 8x16, A via LDS.64 pipe
-using W2 = Cfg<128, 128, 4, 1, 16, 3, kLoaderTma, 2, 8, 1>;  // 4 warps x 2 CTAs/SM
-using W3 = Cfg<128, 128, 4, 1, 16, 3, kLoaderTma, 2, 8, 2>;
+using C0 = Cfg<128, 256, 4, 2, 16, 4, kLoaderTma, 1>;        // 8 warps, 192 KB smem, 1/SM
+using C1 = Cfg<128, 128, 4, 2, 8, 3, kLoaderTma, 2>;         // 8 warps,  96 KB, 2/SM
+using C2 = Cfg<128, 128, 4, 1, 16, 3, kLoaderTma, 2>;        // 4 warps,  96 KB, 2/SM
+using C3 = Cfg<64, 128, 2, 2, 8, 4, kLoaderTma, 2>;          // 4 warps,  96 KB, 2/SM
+using C4 = Cfg<64, 64, 2, 1, 8, 4, kLoaderTma, 3>;           // 2 warps,  64 KB, 3/SM
+using C5 = Cfg<64, 128, 2, 2, 8, 3, kLoaderTma, 3>;          // 4 warps,  72 KB, 3/SM
+using C6 = Cfg<128, 64, 4, 1, 8, 3, kLoaderTma, 3>;          // 4 warps,  72 KB, 3/SM
+// Rolled core: 4 four-deep steps per loop iteration, double-buffered fragments.
+using R0 = Cfg<128, 256, 4, 2, 16, 4, kLoaderTma, 1, 4, 3>;
+using R1 = Cfg<128, 128, 4, 1, 16, 3, kLoaderTma, 2, 4, 3>;
+using R2 = Cfg<128, 64, 4, 1, 8, 3, kLoaderTma, 3, 4, 3>;
+using R3 = Cfg<64, 128, 2, 2, 8, 3, kLoaderTma, 3, 4, 3>;
 using C8 = Cfg<128, 256, 4, 2, 16, 4, kLoaderAsync4, 1>;
 using C9 = Cfg<128, 128, 4, 2, 8, 3, kLoaderAsync4, 2>;
-using C10 = Cfg<128, 128, 4, 1, 16, 3, kLoaderAsync4, 2>;
 using C11 = Cfg<64, 128, 2, 2, 8, 4, kLoaderAsync4, 2>;
 using C12 = Cfg<64, 64, 2, 1, 8, 4, kLoaderAsync4, 3>;
-using C13 = Cfg<64, 128, 2, 2, 8, 3, kLoaderAsync4, 3>;
 using C14 = Cfg<128, 64, 4, 1, 8, 3, kLoaderAsync4, 3>;
-using C15 = Cfg<64, 128, 2, 2, 8, 4, kLoaderAsync4, 2, 2>;
-using C15p = Cfg<64, 128, 2, 2, 8, 4, kLoaderAsync4, 2, 8, 1>;
-using C15q = Cfg<128, 128, 4, 2, 8, 3, kLoaderAsync4, 1, 8, 1>;
+using R5 = Cfg<128, 128, 4, 1, 16, 3, kLoaderAsync4, 2, 4, 3>;
+using R6 = Cfg<128, 64, 4, 1, 8, 3, kLoaderAsync4, 3, 4, 3>;
 
 struct ConfigDesc {
     const char* name;
@@ -54,18 +49,15 @@ constexpr ConfigDesc describe(const char* name, float eff) {
 // Efficiencies: GFLOP/s measured on a B200 at 8192^3 (alpha=1.5, beta=0.5),
 // normalised to the best configuration of the same loader.
 static const ConfigDesc kConfigs[] = {
-    describe<C0>("tma_128x256_w8_t8x16_s4", 0.956f),  describe<C1>("tma_128x128_w8_t8x8_s3", 0.99f),
-    describe<C2>("tma_128x128_w4_t8x16_s3", 0.95f),   describe<C3>("tma_64x128_w4_t8x8_s4", 1.00f),
-    describe<C4>("tma_64x64_w2_t8x8_s4", 0.88f),      describe<C5>("tma_64x128_w4_t8x8_s3", 0.98f),
-    describe<C6>("tma_128x64_w4_t8x8_s3", 0.97f),     describe<C7>("tma_64x128_w4_t8x8_s4_u2", 0.97f),
-    describe<C7p>("tma_64x128_w4_t8x8_s4_pipe", 0.97f), describe<C7q>("tma_128x128_w8_t8x8_s3_pipe", 0.97f),
-    describe<W0>("tma_128x256_w8_t8x16_s4_pipe", 0.95f), describe<W1>("tma_128x256_w8_t8x16_s4_p64", 0.95f),
-    describe<W2>("tma_128x128_w4_t8x16_s3_pipe", 0.95f), describe<W3>("tma_128x128_w4_t8x16_s3_p64", 0.95f),
-    describe<C8>("cpa_128x256_w8_t8x16_s4", 0.75f),   describe<C9>("cpa_128x128_w8_t8x8_s3", 0.71f),
-    describe<C10>("cpa_128x128_w4_t8x16_s3", 0.72f),  describe<C11>("cpa_64x128_w4_t8x8_s4", 0.64f),
-    describe<C12>("cpa_64x64_w2_t8x8_s4", 0.50f),     describe<C13>("cpa_64x128_w4_t8x8_s3", 0.62f),
-    describe<C14>("cpa_128x64_w4_t8x8_s3", 0.62f),    describe<C15>("cpa_64x128_w4_t8x8_s4_u2", 0.62f),
-    describe<C15p>("cpa_64x128_w4_t8x8_s4_pipe", 0.62f), describe<C15q>("cpa_128x128_w8_t8x8_s3_pipe", 0.62f),
+    describe<C0>("tma_128x256_w8_t8x16_s4", 0.95f),    describe<C1>("tma_128x128_w8_t8x8_s3", 0.96f),
+    describe<C2>("tma_128x128_w4_t8x16_s3", 0.95f),    describe<C3>("tma_64x128_w4_t8x8_s4", 0.96f),
+    describe<C4>("tma_64x64_w2_t8x8_s4", 0.82f),       describe<C5>("tma_64x128_w4_t8x8_s3", 0.97f),
+    describe<C6>("tma_128x64_w4_t8x8_s3", 0.99f),      describe<R0>("tma_128x256_w8_t8x16_s4_r4", 0.99f),
+    describe<R1>("tma_128x128_w4_t8x16_s3_r4", 1.00f), describe<R2>("tma_128x64_w4_t8x8_s3_r4", 1.00f),
+    describe<R3>("tma_64x128_w4_t8x8_s3_r4", 0.99f),   describe<C8>("cpa_128x256_w8_t8x16_s4", 0.62f),
+    describe<C9>("cpa_128x128_w8_t8x8_s3", 0.62f),     describe<C11>("cpa_64x128_w4_t8x8_s4", 0.55f),
+    describe<C12>("cpa_64x64_w2_t8x8_s4", 0.43f),      describe<C14>("cpa_128x64_w4_t8x8_s3", 0.59f),
+    describe<R5>("cpa_128x128_w4_t8x16_s3_r4", 0.62f), describe<R6>("cpa_128x64_w4_t8x8_s3_r4", 0.62f),
 };
 constexpr int kNumConfigs = sizeof(kConfigs) / sizeof(kConfigs[0]);
 
@@ -135,11 +127,67 @@ int plain_select(int m, int n, int k, const float* A, int lda, const float* B, i
     return best;
 }
 
+namespace ffma {
+
+// Row copy into a 16-byte-aligned pitch (the pack step for strides TMA cannot
+// describe).
+__global__ void pack_rows_kernel(const float* __restrict__ src, int rows, int cols, int ld_src,
+                                 float* __restrict__ dst, int ld_dst) {
+    const int64_t total = (int64_t)rows * cols;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t r = i / cols, c = i % cols;
+        dst[r * ld_dst + c] = src[r * ld_src + c];
+    }
+}
+
+// Work (m*n*k) above which copying unaligned operands to aligned rows and
+// running the TMA kernel beats the 4-byte cp.async loader.
+constexpr double kPackMinWork = 134217728.0;  // 512^3
+
+static void pack(const float* src, int rows, int cols, int ld_src, float* dst, int ld_dst,
+                 cudaStream_t s) {
+    const int64_t total = (int64_t)rows * cols;
+    int64_t blocks = (total + 255) / 256;
+    if (blocks > 148 * 32) blocks = 148 * 32;
+    pack_rows_kernel<<<(int)blocks, 256, 0, s>>>(src, rows, cols, ld_src, dst, ld_dst);
+}
+
+}  // namespace ffma
+
 int plain_launch(int cfg, int m, int n, int k, float alpha, const float* A, int lda,
                  const float* B, int ldb, float beta, float* C, int ldc, cudaStream_t stream) {
     using namespace ffma;
     if (m == 0 || n == 0) return SGEMM_B200_OK;
     if (!device_is_sm100()) return SGEMM_B200_ERR_UNSUPPORTED;
+    if (cfg < 0 && k > 0 && !tma_ok(A, lda, B, ldb) && double(m) * n * k >= kPackMinWork) {
+        // Unaligned strides on a large problem: copy the offending operand(s) to
+        // 16-byte-aligned rows (stream-ordered scratch from the library pool)
+        // and run the TMA kernel.  Same arithmetic, same bits.
+        cudaMemPool_t pool = library_pool();
+        if (pool) {
+            const bool pa = (lda % 4 != 0) || (reinterpret_cast<uintptr_t>(A) % 16 != 0);
+            const bool pb = (ldb % 4 != 0) || (reinterpret_cast<uintptr_t>(B) % 16 != 0);
+            const int lda2 = pa ? (k + 3) / 4 * 4 : lda, ldb2 = pb ? (n + 3) / 4 * 4 : ldb;
+            float *A2 = nullptr, *B2 = nullptr;
+            cudaError_t e = cudaSuccess;
+            if (pa) e = cudaMallocFromPoolAsync(&A2, sizeof(float) * (size_t)m * lda2, pool, stream);
+            if (e == cudaSuccess && pb)
+                e = cudaMallocFromPoolAsync(&B2, sizeof(float) * (size_t)k * ldb2, pool, stream);
+            if (e == cudaSuccess) {
+                if (pa) pack(A, m, k, lda, A2, lda2, stream);
+                if (pb) pack(B, k, n, ldb, B2, ldb2, stream);
+                const int s = plain_launch(-1, m, n, k, alpha, pa ? A2 : A, lda2, pb ? B2 : B,
+                                           ldb2, beta, C, ldc, stream);
+                if (A2) cudaFreeAsync(A2, stream);
+                if (B2) cudaFreeAsync(B2, stream);
+                return s;
+            }
+            if (A2) cudaFreeAsync(A2, stream);
+            if (B2) cudaFreeAsync(B2, stream);
+            cudaGetLastError();  // fall through to the cp.async loader
+        }
+    }
     if (cfg < 0) cfg = plain_select(m, n, k, A, lda, B, ldb);
     if (cfg >= kNumConfigs) return SGEMM_B200_ERR_INVALID_ARG;
     const ConfigDesc& cd = kConfigs[cfg];

@@ -41,7 +41,9 @@ struct Cfg {
     static constexpr int LOADER = LOADER_;
     static constexpr int MINB = MINB_;  // resident CTAs per SM the register budget targets
     static constexpr int K4U = K4U_;    // unroll of the 8 four-deep k steps of a k block
-    static constexpr int PIPE = PIPE_;  // 1: double-buffered LDS.128 fragments, 2: A via LDS.64
+    // 0: fully unrolled, compiler-scheduled; 1: double-buffered LDS.128 fragments;
+    // 2: A via LDS.64; 3: rolled loop of K4U four-deep steps, double-buffered
+    static constexpr int PIPE = PIPE_;
     static constexpr int BK = 32;  // one 128-byte row of A per k block
     static constexpr int TM = 8;
     static constexpr int THREADS = 32 * WM * WN;
@@ -174,6 +176,53 @@ __device__ __forceinline__ void compute_stage_pipelined64(const uint8_t* __restr
     }
 }
 
+// Compact pipelined core: the 8 four-deep steps of a k block run as a rolled
+// loop of 8 / G iterations with G steps unrolled in each, so the loop body
+// (G x 4 x TM x TN FFMAs) stays small enough for the instruction cache; the
+// fragment double buffering continues across iterations, with the loads past
+// the end of the block predicated off.
+template <class C>
+__device__ __forceinline__ void compute_stage_rolled(const uint8_t* __restrict__ As,
+                                                     const uint8_t* __restrict__ Bs,
+                                                     uint32_t a_base, uint32_t xa0, uint32_t xa1,
+                                                     uint32_t b_base, float (&acc)[C::TM][C::TN]) {
+    constexpr int G = C::K4U;  // four-deep steps per loop iteration: even, so the
+    static_assert(G == 2 || G == 4, "");  // double-buffer slots stay compile-time
+    constexpr int NK4 = C::BK / 4;
+    float4 a[2][C::TM];
+    float4 b[2][C::TN / 4];
+    load_a_frag<C>(As, a_base, xa0, xa1, 0, a[0]);
+    load_b_frag<C>(Bs, b_base, 0, b[0]);
+#pragma unroll 1
+    for (int it = 0; it < NK4 / G; ++it) {
+#pragma unroll
+        for (int u = 0; u < G; ++u) {
+            const int k4 = it * G + u;
+#pragma unroll
+            for (int kk = 0; kk < 4; ++kk) {
+                const int k = 4 * k4 + kk;
+                const int bufa = u & 1;  // k4 & 1, since it * G is even
+                if (kk == 0 && k4 + 1 < NK4) load_a_frag<C>(As, a_base, xa0, xa1, k4 + 1, a[bufa ^ 1]);
+                if (k + 1 < C::BK) load_b_frag<C>(Bs, b_base, k + 1, b[(kk + 1) & 1]);
+                const float4(&ac)[C::TM] = a[bufa];
+                const float4(&bc)[C::TN / 4] = b[kk & 1];
+#pragma unroll
+                for (int i = 0; i < C::TM; ++i) {
+                    const float av =
+                        kk == 0 ? ac[i].x : kk == 1 ? ac[i].y : kk == 2 ? ac[i].z : ac[i].w;
+#pragma unroll
+                    for (int g = 0; g < C::TN / 4; ++g) {
+                        acc[i][4 * g + 0] = fmaf(av, bc[g].x, acc[i][4 * g + 0]);
+                        acc[i][4 * g + 1] = fmaf(av, bc[g].y, acc[i][4 * g + 1]);
+                        acc[i][4 * g + 2] = fmaf(av, bc[g].z, acc[i][4 * g + 2]);
+                        acc[i][4 * g + 3] = fmaf(av, bc[g].w, acc[i][4 * g + 3]);
+                    }
+                }
+            }
+        }
+    }
+}
+
 // Fragment-at-a-time core: A for a 4-deep step at its start, B per k (the
 // compiler schedules the loads).
 template <class C>
@@ -221,6 +270,8 @@ __device__ __forceinline__ void compute_stage(const uint8_t* __restrict__ As,
                                               float (&acc)[C::TM][C::TN]) {
     if constexpr (C::PIPE == 1)
         compute_stage_pipelined<C>(As, Bs, a_base, xa0, xa1, b_base, acc);
+    else if constexpr (C::PIPE == 3)
+        compute_stage_rolled<C>(As, Bs, a_base, xa0, xa1, b_base, acc);
     else if constexpr (C::PIPE == 2)
         compute_stage_pipelined64<C>(As, Bs, a_base, xa0, xa1, b_base, acc);
     else

@@ -7,12 +7,12 @@
 // Design:
 //  - The plan flattens every problem into work items (tile_m, tile_n, k
 //    split), sorted longest-first so the tail of the launch is short items.
-//  - One persistent CTA per SM (256 threads) claims items with an atomic
-//    counter and runs the same FFMA core as the plain path on each: one of two
-//    tile shapes (128x256 with 8x16 thread tiles, or 128x128 with 8x8) and one
-//    of two loaders (TMA with per-problem tensor maps kept in global memory,
-//    or 4-byte cp.async for strides TMA cannot describe), all chosen per
-//    problem at plan time.
+//  - Persistent 4-warp CTAs (2 or 3 per SM) claim items with an atomic
+//    counter and run the same FFMA core as the plain path on each: one of two
+//    tile shapes (128x64 or 64x128, 8 x 8 thread tiles) and one of two
+//    loaders (TMA with per-problem tensor maps kept in global memory, or
+//    4-byte cp.async for strides TMA cannot describe), chosen per problem at
+//    plan time.
 //  - Items with split == 1 run the plain path's exact arithmetic, so their
 //    results equal sgemm_b200's bit for bit.  Split-K items write partial sums
 //    to a workspace; the last split of a tile to finish (atomic ticket) adds
@@ -42,18 +42,25 @@ namespace grouped {
 
 using ffma::Operands;
 
+// Two tile shapes of the plain path's 4-warp, 8 x 8 thread-tile FFMA core
+// share one kernel (same thread count, same 24 KB stage, ~168 registers):
+// 3 stages fit 3 CTAs per SM, 4 stages fit 2.
 template <int S>
-using CfgL = ffma::Cfg<128, 256, 4, 2, 16, S, ffma::kLoaderTma, 1>;
+using CfgT = ffma::Cfg<128, 64, 4, 1, 8, S, ffma::kLoaderTma, (S == 3 ? 3 : 2)>;  // 128 x 64
 template <int S>
-using CfgM = ffma::Cfg<128, 128, 4, 2, 8, S, ffma::kLoaderTma, 1>;
+using CfgW = ffma::Cfg<64, 128, 2, 2, 8, S, ffma::kLoaderTma, (S == 3 ? 3 : 2)>;  // 64 x 128
 
-constexpr int THREADS = 256;
-constexpr int SLOT_BYTES = 128 * 32 * 4 + 32 * 256 * 4;  // largest stage (128x256): 48 KB
-enum TileShape { kTileL = 0, kTileM = 1 };
+constexpr int THREADS = 128;
+constexpr int SLOT_BYTES = 24 * 1024;  // both shapes: 16 KB + 8 KB per 32-deep k block
+static_assert(CfgT<3>::STAGE_BYTES == SLOT_BYTES && CfgW<3>::STAGE_BYTES == SLOT_BYTES, "");
+enum TileShape { kTileTall = 0, kTileWide = 1 };  // 128 x 64, 64 x 128
+
+inline int tile_bm(int t) { return t == kTileTall ? 128 : 64; }
+inline int tile_bn(int t) { return t == kTileTall ? 64 : 128; }
 
 struct GProblem {
     Operands op;
-    int tile;      // kTileL or kTileM
+    int tile;      // kTileTall or kTileWide
     int tma;       // tensor maps valid
     int split;     // k splits
     int kbps;      // k blocks per split
@@ -221,7 +228,7 @@ __device__ __forceinline__ bool run_item(const GParams& gp, const GProblem& pr, 
 }
 
 template <int S>
-__global__ void __launch_bounds__(THREADS, 1) grouped_kernel(const GParams gp) {
+__global__ void __launch_bounds__(THREADS, (S == 3 ? 3 : 2)) grouped_kernel(const GParams gp) {
     extern __shared__ uint8_t smem_raw[];
     __shared__ __align__(8) uint64_t full_bar[S];
     __shared__ int item_s;
@@ -242,13 +249,13 @@ __global__ void __launch_bounds__(THREADS, 1) grouped_kernel(const GParams gp) {
         const GItem it = gp.items[idx];
         const GProblem& pr = gp.probs[it.prob];
         bool ok;
-        if (pr.tile == kTileL) {
-            ok = pr.tma ? run_item<CfgL<S>, true, S>(gp, pr, it, it.prob, smem, full_bar, g, &last_s)
-                        : run_item<CfgL<S>, false, S>(gp, pr, it, it.prob, smem, full_bar, g,
+        if (pr.tile == kTileTall) {
+            ok = pr.tma ? run_item<CfgT<S>, true, S>(gp, pr, it, it.prob, smem, full_bar, g, &last_s)
+                        : run_item<CfgT<S>, false, S>(gp, pr, it, it.prob, smem, full_bar, g,
                                                       &last_s);
         } else {
-            ok = pr.tma ? run_item<CfgM<S>, true, S>(gp, pr, it, it.prob, smem, full_bar, g, &last_s)
-                        : run_item<CfgM<S>, false, S>(gp, pr, it, it.prob, smem, full_bar, g,
+            ok = pr.tma ? run_item<CfgW<S>, true, S>(gp, pr, it, it.prob, smem, full_bar, g, &last_s)
+                        : run_item<CfgW<S>, false, S>(gp, pr, it, it.prob, smem, full_bar, g,
                                                       &last_s);
         }
         if (!ok) break;
@@ -259,7 +266,7 @@ __global__ void __launch_bounds__(THREADS, 1) grouped_kernel(const GParams gp) {
 // ------------------------------------------------------------------ host --
 
 struct Choice {
-    int tile = kTileM;
+    int tile = kTileTall;
     int split = 1;
 };
 
@@ -279,7 +286,7 @@ struct Table {
         for (int a = 0; a < kMnClasses; ++a)
             for (int b = 0; b < kKClasses; ++b) {
                 Choice& ch = c[a * kKClasses + b];
-                ch.tile = a == 2 ? kTileL : kTileM;
+                ch.tile = kTileTall;
                 ch.split = 1;
             }
     }
@@ -429,7 +436,7 @@ static int make_schedule(const sgemm_b200_problem* probs, int count, const Table
         g.op.vec_c = (q.ldc % 4 == 0) && (reinterpret_cast<uintptr_t>(q.C) % 16 == 0);
         const Choice ch = table.c[bucket_of(q.m, q.n, q.k)];
         g.tile = ch.tile;
-        const int bm = 128, bn = ch.tile == kTileL ? 256 : 128;
+        const int bm = tile_bm(ch.tile), bn = tile_bn(ch.tile);
         g.tma = tma_ok(q) ? 1 : 0;
         const int nk = div_up(q.k, 32);
         int split = std::max(1, std::min(ch.split, nk));
@@ -470,6 +477,17 @@ static void set_kernel_attributes() {
                          smem_bytes<4>());
 }
 
+// Persistent CTAs per SM of the kernel variant with `stages` stages.
+static int resident_per_sm(int stages) {
+    int occ = 0;
+    const cudaError_t e =
+        stages == 3 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, grouped_kernel<3>,
+                                                                    THREADS, smem_bytes<3>())
+                    : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, grouped_kernel<4>,
+                                                                    THREADS, smem_bytes<4>());
+    return (e == cudaSuccess && occ > 0) ? occ : 1;
+}
+
 static int build_plan(const sgemm_b200_problem* probs, int count, const Table& table,
                       sgemm_b200_grouped_plan** out) {
     if (!out) return SGEMM_B200_ERR_INVALID_ARG;
@@ -490,10 +508,10 @@ static int build_plan(const sgemm_b200_problem* probs, int count, const Table& t
     for (int i = 0; i < count; ++i) {
         const GProblem& g = sc.probs[i];
         if (!g.tma) continue;
-        const int bn = g.tile == kTileL ? 256 : 128;
+        const int bm = tile_bm(g.tile), bn = tile_bn(g.tile);
         if (!encode_tensor_map_2d(&maps[2 * i], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, g.op.A,
                                   (uint64_t)g.op.k, (uint64_t)g.op.m, (uint64_t)g.op.lda * 4, 32,
-                                  128, CU_TENSOR_MAP_SWIZZLE_128B) ||
+                                  bm, CU_TENSOR_MAP_SWIZZLE_128B) ||
             !encode_tensor_map_2d(&maps[2 * i + 1], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, g.op.B,
                                   (uint64_t)g.op.n, (uint64_t)g.op.k, (uint64_t)g.op.ldb * 4, bn,
                                   32, CU_TENSOR_MAP_SWIZZLE_NONE)) {
@@ -527,7 +545,7 @@ static int build_plan(const sgemm_b200_problem* probs, int count, const Table& t
     }
     set_kernel_attributes();
     const int sms = device_info().sm_count;
-    plan->grid = std::max(1, std::min(sms, plan->n_items));
+    plan->grid = std::max(1, std::min(sms * resident_per_sm(plan->stages), plan->n_items));
     *out = plan;
     return SGEMM_B200_OK;
 }
@@ -622,10 +640,10 @@ int arena_launch(Arena* a, const sgemm_b200_problem* probs, int count, cudaStrea
     for (int i = 0; i < count; ++i) {
         const GProblem& g = sc.probs[i];
         if (!g.tma) continue;
-        const int bn = g.tile == kTileL ? 256 : 128;
+        const int bm = tile_bm(g.tile), bn = tile_bn(g.tile);
         if (!encode_tensor_map_2d(&a->h_maps[2 * i], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, g.op.A,
                                   (uint64_t)g.op.k, (uint64_t)g.op.m, (uint64_t)g.op.lda * 4, 32,
-                                  128, CU_TENSOR_MAP_SWIZZLE_128B) ||
+                                  bm, CU_TENSOR_MAP_SWIZZLE_128B) ||
             !encode_tensor_map_2d(&a->h_maps[2 * i + 1], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, g.op.B,
                                   (uint64_t)g.op.n, (uint64_t)g.op.k, (uint64_t)g.op.ldb * 4, bn,
                                   32, CU_TENSOR_MAP_SWIZZLE_NONE))
@@ -653,8 +671,10 @@ int arena_launch(Arena* a, const sgemm_b200_problem* probs, int count, cudaStrea
     p.status = device_status_ptr();
     p.n_items = (int)sc.items.size();
     if (!p.status) return SGEMM_B200_ERR_CUDA;
-    const int grid = std::max(1, std::min(device_info().sm_count, p.n_items));
-    grouped_kernel<4><<<grid, THREADS, smem_bytes<4>(), stream>>>(p);
+    static int per_sm = 0;
+    if (!per_sm) per_sm = resident_per_sm(3);
+    const int grid = std::max(1, std::min(device_info().sm_count * per_sm, p.n_items));
+    grouped_kernel<3><<<grid, THREADS, smem_bytes<3>(), stream>>>(p);
     return cuda_status(cudaGetLastError());
 }
 
@@ -805,7 +825,7 @@ extern "C" int sgemm_b200_autotune_grouped(const sgemm_b200_problem* problems, i
     for (int b = 0; b < kBuckets; ++b) {
         if (!present[b]) continue;
         const int kclass = b % kKClasses;
-        for (int tile : {kTileL, kTileM})
+        for (int tile : {kTileTall, kTileWide})
             for (int split : {1, 2, 4, 8}) {
                 if (split > 1 && kclass == 0) continue;
                 Table t = best;

@@ -12,28 +12,27 @@
 // TF32X3: x_h = tf32(x), x_l = tf32(x - x_h);  A*B = hh + (hl + lh).
 //
 // The products run as tcgen05.mma (kind::f16 with BF16 inputs, or
-// kind::tf32) with FP32 accumulation in tensor memory.  Two things keep the
-// result as accurate as the FP32 FFMA path:
-//  - the dominant hh term and the small correction terms accumulate in
-//    separate TMEM accumulators (D1, D2), so the corrections' rounding is
-//    ~2^-8 smaller than the main sum's;
-//  - the tensor core only ever accumulates one K chunk (KCHUNK = 128) into a
-//    TMEM buffer; eight drain warps then add that chunk's D1 + D2 into FP32
-//    registers with round-to-nearest while the MMA warp fills the other
-//    buffer.  Long accumulations inside the tensor core lose accuracy with
-//    K; chunk sums added on the CUDA cores do not.
+// kind::tf32) with FP32 accumulation in tensor memory.  Accuracy:
+//  - the dominant hh term (D1) and the correction terms (D2) accumulate in
+//    separate TMEM accumulators;
+//  - D1 only ever accumulates one K chunk (KCHUNK) in the tensor core: eight
+//    drain warps then add the chunk into FP32 registers with round-to-nearest
+//    before the next chunk overwrites D1.  Long accumulations inside the
+//    tensor core lose accuracy with K; chunk sums added on the CUDA cores do
+//    not.  D2 is ~2^-8 of D1, so its own accumulation error is negligible and
+//    it is read once, at the end;
+//  - every k step issues its correction MMAs before its hh MMA, so while the
+//    drain warps empty D1 the tensor core still has the next step's
+//    corrections to work on.
 //
-// Kernel shape: one CTA of 10 warps per 128 x 128 output tile.
+// Kernel shape: one CTA of 10 warps per 128 x 256 output tile.
 //   warps 0..7  drain + epilogue: warp w reads TMEM lanes 32*(w%4).. (rows)
-//               and columns 64*(w/4)..+63 of each chunk, keeps 64 FP32
-//               running sums, and finally applies alpha/beta and stores
-//               float4s
+//               and columns 128*(w/4)..+127, keeps 128 FP32 running sums,
+//               and finally adds D2, applies alpha/beta and stores float4s
 //   warp 8      TMA producer (one lane): one 3-D box per operand per stage
 //               brings every split plane of a 64-byte K slice (64-byte swizzle)
-//   warp 9      MMA issuer (one lane): tcgen05.mma M=128 N=128; commit per
-//               stage frees the stage, commit per chunk hands the chunk's
-//               TMEM buffer to the drain warps
-// TMEM (512 columns): buffer b in {0,1} holds D1 at 256b and D2 at 256b+128.
+//   warp 9      MMA issuer (one lane): tcgen05.mma M=128 N=256
+// TMEM (512 columns): D1 at 0, D2 at 256.
 // Every mbarrier wait is bounded (ptx.cuh); on expiry the status word is
 // set, in-flight copies are drained with bounded waits and TMEM is freed.
 //
@@ -51,36 +50,36 @@
 namespace sgb {
 namespace split {
 
-constexpr int BM = 128, BN = 128;
+constexpr int BM = 128, BN = 256;
 constexpr int DRAIN_WARPS = 8, PRODUCER_WARP = 8, MMA_WARP = 9;
 constexpr int THREADS = 32 * (DRAIN_WARPS + 2);
 constexpr int TMEM_COLS = 512;
-constexpr int KCHUNK = 128;  // K depth one TMEM accumulation spans
+constexpr int KCHUNK = 256;  // K depth D1 accumulates in the tensor core before a drain
 
 template <int PATH>
 struct Traits;
 
 template <>
 struct Traits<SGEMM_B200_PATH_BF16X6> {
-    static constexpr int NSPLIT = 3, ESZ = 2, BK = 32, KMMA = 16, STAGES = 4;
+    static constexpr int NSPLIT = 3, ESZ = 2, BK = 32, KMMA = 16, STAGES = 3;
     static constexpr uint32_t FMT = 1;  // BF16
     static constexpr int NPROD = 6;
-    // (a split, b split) in issue order: hh first (D1), then the corrections (D2)
+    // (a split, b split) in issue order: the corrections (D2) first, hh (D1) last
     __device__ static constexpr int pa(int i) {
-        return i == 0 ? 0 : i == 1 ? 0 : i == 2 ? 1 : i == 3 ? 0 : i == 4 ? 2 : 1;
+        return i == 0 ? 0 : i == 1 ? 1 : i == 2 ? 0 : i == 3 ? 2 : i == 4 ? 1 : 0;
     }
     __device__ static constexpr int pb(int i) {
-        return i == 0 ? 0 : i == 1 ? 1 : i == 2 ? 0 : i == 3 ? 2 : i == 4 ? 0 : 1;
+        return i == 0 ? 1 : i == 1 ? 0 : i == 2 ? 2 : i == 3 ? 0 : i == 4 ? 1 : 0;
     }
 };
 
 template <>
 struct Traits<SGEMM_B200_PATH_TF32X3> {
-    static constexpr int NSPLIT = 2, ESZ = 4, BK = 16, KMMA = 8, STAGES = 6;
+    static constexpr int NSPLIT = 2, ESZ = 4, BK = 16, KMMA = 8, STAGES = 4;
     static constexpr uint32_t FMT = 2;  // TF32
     static constexpr int NPROD = 3;
-    __device__ static constexpr int pa(int i) { return i == 2 ? 1 : 0; }
-    __device__ static constexpr int pb(int i) { return i == 1 ? 1 : 0; }
+    __device__ static constexpr int pa(int i) { return i == 1 ? 1 : 0; }
+    __device__ static constexpr int pb(int i) { return i == 0 ? 1 : 0; }
 };
 
 template <int PATH>
@@ -89,12 +88,13 @@ struct Layout {
     static constexpr int ROW_BYTES = T::BK * T::ESZ;  // 64: one swizzle-64 row
     static_assert(ROW_BYTES == 64, "64-byte K rows");
     static constexpr int A_PLANE = BM * ROW_BYTES;    // 8 KB
-    static constexpr int B_PLANE = BN * ROW_BYTES;    // 8 KB
+    static constexpr int B_PLANE = BN * ROW_BYTES;    // 16 KB
     static constexpr int A_BYTES = T::NSPLIT * A_PLANE;
     static constexpr int B_BYTES = T::NSPLIT * B_PLANE;
     static constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
     static constexpr int SMEM_BYTES = T::STAGES * STAGE_BYTES + 1024;
-    static constexpr int CHUNK_STAGES = KCHUNK / T::BK;
+    static constexpr int STEPS = T::BK / T::KMMA;           // MMA k steps per stage
+    static constexpr int CHUNK_STEPS = KCHUNK / T::KMMA;    // k steps per D1 chunk
     static_assert(KCHUNK % T::BK == 0, "whole stages per chunk");
     static_assert(SMEM_BYTES <= 227 * 1024, "shared memory budget");
 };
@@ -129,8 +129,8 @@ __global__ void __launch_bounds__(THREADS, 1)
     extern __shared__ uint8_t smem_raw[];
     __shared__ __align__(8) uint64_t full_bar[T::STAGES];
     __shared__ __align__(8) uint64_t empty_bar[T::STAGES];
-    __shared__ __align__(8) uint64_t filled_bar[2];
-    __shared__ __align__(8) uint64_t drained_bar[2];
+    __shared__ __align__(8) uint64_t d1_full_bar;
+    __shared__ __align__(8) uint64_t d1_empty_bar;
     __shared__ uint32_t tmem_base_s;
     __shared__ volatile int abort_s;
     __shared__ int consumed_s;
@@ -141,17 +141,16 @@ __global__ void __launch_bounds__(THREADS, 1)
     tile_coords(blockIdx.x, p.tiles_m, p.tiles_n, tm, tn);
     const int m0 = tm * BM, n0 = tn * BN;
     const int nk = (p.k + T::BK - 1) / T::BK;
-    const int nchunks = (nk + L::CHUNK_STAGES - 1) / L::CHUNK_STAGES;
+    const int nsteps = nk * L::STEPS;
+    const int nchunks = (nsteps + L::CHUNK_STEPS - 1) / L::CHUNK_STEPS;
 
     if (tid == 0) {
         for (int s = 0; s < T::STAGES; ++s) {
             mbar_init(&full_bar[s], 1);
             mbar_init(&empty_bar[s], 1);
         }
-        for (int b = 0; b < 2; ++b) {
-            mbar_init(&filled_bar[b], 1);
-            mbar_init(&drained_bar[b], DRAIN_WARPS);
-        }
+        mbar_init(&d1_full_bar, 1);
+        mbar_init(&d1_empty_bar, DRAIN_WARPS);
         abort_s = 0;
         consumed_s = 0;
         fence_barrier_init();
@@ -166,7 +165,6 @@ __global__ void __launch_bounds__(THREADS, 1)
     const uint32_t tmem = tmem_base_s;
 
     int issued = 0;
-    float acc[64];
     if (warp == PRODUCER_WARP) {
         if (lane == 0) {
             // ------------------------------------------------ TMA producer --
@@ -192,49 +190,57 @@ __global__ void __launch_bounds__(THREADS, 1)
         if (lane == 0) {
             // -------------------------------------------------- MMA issuer --
             constexpr uint32_t idesc = make_idesc(T::FMT, BM, BN);
+            const uint32_t d1 = tmem, d2 = tmem + static_cast<uint32_t>(BN);
             int kb = 0;
             bool ok = true;
-            for (int c = 0; c < nchunks && ok; ++c) {
-                const int b = c & 1;
-                if (c >= 2 && (!mbar_wait(&drained_bar[b], ((c >> 1) - 1) & 1) || abort_s)) {
+            for (; kb < nk && ok; ++kb) {
+                const int s = kb % T::STAGES;
+                if (!mbar_wait(&full_bar[s], (kb / T::STAGES) & 1) || abort_s) {
                     ok = false;
                     break;
                 }
                 tc_fence_after();
-                const uint32_t d1 = tmem + static_cast<uint32_t>(b * 256);
-                const int kend = min(nk, (c + 1) * L::CHUNK_STAGES);
-                for (; kb < kend; ++kb) {
-                    const int s = kb % T::STAGES;
-                    if (!mbar_wait(&full_bar[s], (kb / T::STAGES) & 1) || abort_s) {
-                        ok = false;
-                        break;
+                const uint32_t a0 = smem_u32(smem + s * L::STAGE_BYTES);
+                const uint32_t b0 = a0 + L::A_BYTES;
+#pragma unroll
+                for (int j = 0; j < L::STEPS; ++j) {
+                    const int step = kb * L::STEPS + j;
+                    const uint32_t koff = j * T::KMMA * T::ESZ;  // 32 B per MMA K slice
+                    // corrections into D2 (accumulated over the whole K)
+#pragma unroll
+                    for (int i = 0; i < T::NPROD - 1; ++i) {
+                        const uint64_t ad = sw64_kmajor_desc(a0 + T::pa(i) * L::A_PLANE + koff);
+                        const uint64_t bd = sw64_kmajor_desc(b0 + T::pb(i) * L::B_PLANE + koff);
+                        const uint32_t accum = (step > 0 || i > 0) ? 1u : 0u;
+                        if constexpr (T::FMT == 1)
+                            mma_bf16_ss(d2, ad, bd, idesc, accum);
+                        else
+                            mma_tf32_ss(d2, ad, bd, idesc, accum);
                     }
-                    tc_fence_after();
-                    const uint32_t a0 = smem_u32(smem + s * L::STAGE_BYTES);
-                    const uint32_t b0 = a0 + L::A_BYTES;
-                    const bool chunk_start = kb == c * L::CHUNK_STAGES;
-#pragma unroll
-                    for (int j = 0; j < T::BK / T::KMMA; ++j) {
-                        const uint32_t koff = j * T::KMMA * T::ESZ;  // 32 B per MMA K slice
-#pragma unroll
-                        for (int i = 0; i < T::NPROD; ++i) {
-                            const uint64_t ad =
-                                sw64_kmajor_desc(a0 + T::pa(i) * L::A_PLANE + koff);
-                            const uint64_t bd =
-                                sw64_kmajor_desc(b0 + T::pb(i) * L::B_PLANE + koff);
-                            const uint32_t d = d1 + (i == 0 ? 0u : static_cast<uint32_t>(BN));
-                            // the first product into each accumulator of a chunk overwrites it
-                            const uint32_t accum = (chunk_start && j == 0 && i <= 1) ? 0u : 1u;
-                            if constexpr (T::FMT == 1)
-                                mma_bf16_ss(d, ad, bd, idesc, accum);
-                            else
-                                mma_tf32_ss(d, ad, bd, idesc, accum);
+                    // hh into D1, which restarts every chunk once the drain emptied it
+                    const int c = step / L::CHUNK_STEPS;
+                    const bool chunk_start = step % L::CHUNK_STEPS == 0;
+                    if (chunk_start && c > 0) {
+                        if (!mbar_wait(&d1_empty_bar, (c - 1) & 1) || abort_s) {
+                            ok = false;
+                            break;
                         }
+                        tc_fence_after();
                     }
-                    mma_commit(&empty_bar[s]);  // frees the stage once these MMAs read it
+                    {
+                        const int i = T::NPROD - 1;
+                        const uint64_t ad = sw64_kmajor_desc(a0 + T::pa(i) * L::A_PLANE + koff);
+                        const uint64_t bd = sw64_kmajor_desc(b0 + T::pb(i) * L::B_PLANE + koff);
+                        if constexpr (T::FMT == 1)
+                            mma_bf16_ss(d1, ad, bd, idesc, chunk_start ? 0u : 1u);
+                        else
+                            mma_tf32_ss(d1, ad, bd, idesc, chunk_start ? 0u : 1u);
+                    }
+                    if ((step + 1) % L::CHUNK_STEPS == 0 || step + 1 == nsteps)
+                        mma_commit(&d1_full_bar);  // chunk c of D1 (and all MMAs before it) done
                 }
                 if (!ok) break;
-                mma_commit(&filled_bar[b]);  // the chunk's sums are ready in buffer b
+                mma_commit(&empty_bar[s]);  // frees the stage once these MMAs read it
             }
             if (!ok) {
                 abort_s = 1;
@@ -245,64 +251,72 @@ __global__ void __launch_bounds__(THREADS, 1)
     } else {
         // ------------------------------------------------ drain + epilogue --
         const int q = warp & 3, h = warp >> 2;
-        const uint32_t trow = tmem + (static_cast<uint32_t>(q * 32) << 16) + h * 64;
+        const uint32_t trow = tmem + (static_cast<uint32_t>(q * 32) << 16) + h * 128;
+        float acc[128];
 #pragma unroll
-        for (int j = 0; j < 64; ++j) acc[j] = 0.0f;
+        for (int j = 0; j < 128; ++j) acc[j] = 0.0f;
         bool ok = true;
         for (int c = 0; c < nchunks; ++c) {
-            const int b = c & 1;
-            if (!mbar_wait(&filled_bar[b], (c >> 1) & 1) || abort_s) {
+            if (!mbar_wait(&d1_full_bar, c & 1) || abort_s) {
                 ok = false;
                 break;
             }
             tc_fence_after();
 #pragma unroll
-            for (int g = 0; g < 2; ++g) {
-                uint32_t r1[32], r2[32];
-                tmem_ld_32x32b_x32(trow + b * 256 + g * 32, r1);
-                tmem_ld_32x32b_x32(trow + b * 256 + BN + g * 32, r2);
+            for (int g = 0; g < 4; ++g) {
+                uint32_t r[32];
+                tmem_ld_32x32b_x32(trow + g * 32, r);
                 tmem_ld_wait();
 #pragma unroll
                 for (int j = 0; j < 32; ++j)
-                    acc[g * 32 + j] = __fadd_rn(
-                        acc[g * 32 + j], __fadd_rn(__uint_as_float(r1[j]), __uint_as_float(r2[j])));
+                    acc[g * 32 + j] = __fadd_rn(acc[g * 32 + j], __uint_as_float(r[j]));
             }
             tc_fence_before();
             __syncwarp();
-            if (lane == 0) mbar_arrive(&drained_bar[b]);
+            if (lane == 0) mbar_arrive(&d1_empty_bar);
         }
         if (!ok) {
             abort_s = 1;
             atomicExch(p.status, SGEMM_B200_ERR_TIMEOUT);
         } else if (!abort_s) {
+            // D2 is complete: the last D1 commit came after every MMA.
             const int row = m0 + q * 32 + lane;
-            const int col0 = n0 + h * 64;
-            if (row < p.m && col0 < p.n) {
-                float* crow = p.C + (int64_t)row * p.ldc + col0;
-                if (p.vec_c && col0 + 63 < p.n) {
 #pragma unroll
-                    for (int v = 0; v < 16; ++v) {
-                        float4 o = make_float4(__fmul_rn(acc[4 * v], p.alpha),
-                                               __fmul_rn(acc[4 * v + 1], p.alpha),
-                                               __fmul_rn(acc[4 * v + 2], p.alpha),
-                                               __fmul_rn(acc[4 * v + 3], p.alpha));
-                        float4* dst = reinterpret_cast<float4*>(crow + 4 * v);
-                        if (p.beta != 0.0f) {
-                            const float4 old = *dst;
-                            o.x = fmaf(old.x, p.beta, o.x);
-                            o.y = fmaf(old.y, p.beta, o.y);
-                            o.z = fmaf(old.z, p.beta, o.z);
-                            o.w = fmaf(old.w, p.beta, o.w);
+            for (int g = 0; g < 4; ++g) {
+                uint32_t r[32];
+                tmem_ld_32x32b_x32(trow + BN + g * 32, r);
+                tmem_ld_wait();
+                const int col0 = n0 + h * 128 + g * 32;
+                if (row < p.m && col0 < p.n) {
+                    float* crow = p.C + (int64_t)row * p.ldc + col0;
+                    float v[32];
+#pragma unroll
+                    for (int j = 0; j < 32; ++j)
+                        v[j] = __fmul_rn(__fadd_rn(acc[g * 32 + j], __uint_as_float(r[j])),
+                                         p.alpha);
+                    if (p.vec_c && col0 + 31 < p.n) {
+#pragma unroll
+                        for (int t = 0; t < 8; ++t) {
+                            float4 o = make_float4(v[4 * t], v[4 * t + 1], v[4 * t + 2],
+                                                   v[4 * t + 3]);
+                            float4* dst = reinterpret_cast<float4*>(crow + 4 * t);
+                            if (p.beta != 0.0f) {
+                                const float4 old = *dst;
+                                o.x = fmaf(old.x, p.beta, o.x);
+                                o.y = fmaf(old.y, p.beta, o.y);
+                                o.z = fmaf(old.z, p.beta, o.z);
+                                o.w = fmaf(old.w, p.beta, o.w);
+                            }
+                            *dst = o;
                         }
-                        *dst = o;
-                    }
-                } else {
+                    } else {
 #pragma unroll
-                    for (int j = 0; j < 64; ++j) {
-                        if (col0 + j < p.n) {
-                            float o = __fmul_rn(acc[j], p.alpha);
-                            if (p.beta != 0.0f) o = fmaf(crow[j], p.beta, o);
-                            crow[j] = o;
+                        for (int j = 0; j < 32; ++j) {
+                            if (col0 + j < p.n) {
+                                float o = v[j];
+                                if (p.beta != 0.0f) o = fmaf(crow[j], p.beta, o);
+                                crow[j] = o;
+                            }
                         }
                     }
                 }
@@ -502,32 +516,6 @@ static int launch(int m, int n, int k, float alpha, const float* A, int lda, con
 
 }  // namespace split
 
-// Library-owned stream-ordered memory pool for NULL-workspace calls, one per
-// device.  Its release threshold is unlimited, so freed workspaces stay in the
-// pool and the next call reuses them instead of going back to the driver; the
-// caller's default pool is left untouched.
-static cudaMemPool_t workspace_pool() {
-    static cudaMemPool_t pools[64] = {nullptr};
-    static std::mutex mu;
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
-    std::lock_guard<std::mutex> lock(mu);
-    if (!pools[dev]) {
-        cudaMemPoolProps props;
-        std::memset(&props, 0, sizeof(props));
-        props.allocType = cudaMemAllocationTypePinned;
-        props.handleTypes = cudaMemHandleTypeNone;
-        props.location.type = cudaMemLocationTypeDevice;
-        props.location.id = dev;
-        cudaMemPool_t p = nullptr;
-        if (cudaMemPoolCreate(&p, &props) != cudaSuccess) return nullptr;
-        uint64_t threshold = ~0ull;
-        cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &threshold);
-        pools[dev] = p;
-    }
-    return pools[dev];
-}
-
 int split_launch(int path, int m, int n, int k, float alpha, const float* A, int lda,
                  const float* B, int ldb, float beta, float* C, int ldc, void* ws,
                  size_t ws_bytes, cudaStream_t stream) {
@@ -540,7 +528,7 @@ int split_launch(int path, int m, int n, int k, float alpha, const float* A, int
                             : split::workspace_bytes<SGEMM_B200_PATH_TF32X3>(m, n, k);
     bool owned = false;
     if (!ws) {
-        cudaMemPool_t pool = workspace_pool();
+        cudaMemPool_t pool = library_pool();
         if (!pool) return SGEMM_B200_ERR_CUDA;
         cudaError_t e = cudaMallocFromPoolAsync(&ws, need, pool, stream);
         if (e != cudaSuccess) return cuda_status(e);

@@ -17,7 +17,7 @@ def _torch():
     return torch
 
 
-def _table(path, split, tile=1, stages=4):
+def _table(path, split, tile=1, stages=3):
     torch = _torch()
     p = torch.cuda.get_device_properties(0)
     buckets = [{"mn": a, "k": b, "tile": tile, "split": split} for a in range(3) for b in range(3)]

@@ -20,9 +20,8 @@ def test_schedule_default_counts():
     probs = sg.host_problems(shapes)
     s = sg.grouped_schedule(probs)
     tiles = 0
-    for m, n, k in shapes:
-        bn = 256 if m * n >= 1024 * 1024 else 128  # default: 128x256 only for the largest class
-        tiles += math.ceil(m / 128) * math.ceil(n / bn)
+    for m, n, k in shapes:  # default tile: 128 x 64 for every bucket
+        tiles += math.ceil(m / 128) * math.ceil(n / 64)
     assert s["tiles"] == tiles
     assert s["work_items"] == tiles  # no split-K by default: results equal the plain path
     assert s["workspace_bytes"] == 0
