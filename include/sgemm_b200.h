@@ -162,6 +162,36 @@ int sgemm_b200_gemm(int path, int m, int n, int k,
                     sgemm_b200_stream_t stream);
 
 /* ------------------------------------------------------------------------ */
+/* Host-resident operands (no reference counterpart)                         */
+/* ------------------------------------------------------------------------ */
+
+/* C := alpha*A*B + beta*C with A, B and C in HOST memory.  Replaces the
+ * reference callers' cudaMemcpy(A,B,C) -> sgemm() -> cudaMemcpy(C) sequence
+ * (test.cu:70-80, benchmark.cu:69-73): the library stages the operands in
+ * device memory itself, cutting C into blocks (row bands x column chunks,
+ * see sgemm_b200_host_plan) so that the host-to-device copies, the block
+ * GEMMs (four streams) and the device-to-host copies overlap.  `path` is a
+ * sgemm_b200_path; each block is the same GEMM sgemm_b200_gemm() runs, so C
+ * is bit-identical to copying everything and calling it once.  Device memory:
+ * A, B and C, from the library's stream-ordered pool.  Stream-ordered on
+ * `stream`: C on the host is final once `stream` has synchronised.
+ * Page-locked host memory is needed for the overlap (pageable memory works
+ * but copies synchronously).  beta == 0 never reads C.  Not for use inside
+ * CUDA-graph capture.  Returns a sgemm_b200_status; after an error some
+ * blocks of C may be updated. */
+int sgemm_b200_host(int path, int m, int n, int k,
+                    const float* alpha,
+                    const float* A, int lda,
+                    const float* B, int ldb,
+                    const float* beta,
+                    float* C, int ldc,
+                    sgemm_b200_stream_t stream);
+
+/* Block shape sgemm_b200_host uses for this problem: rows per band and
+ * columns per chunk (m and n when it does not split).  Host-only. */
+int sgemm_b200_host_plan(int path, int m, int n, int k, int reads_c, int* rows, int* cols);
+
+/* ------------------------------------------------------------------------ */
 /* Grouped persistent GEMM (no reference counterpart)                        */
 /* ------------------------------------------------------------------------ */
 

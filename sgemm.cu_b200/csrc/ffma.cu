@@ -20,18 +20,14 @@ using C3 = Cfg<64, 128, 2, 2, 8, 4, kLoaderTma, 2>;          // 4 warps,  96 KB,
 using C4 = Cfg<64, 64, 2, 1, 8, 4, kLoaderTma, 3>;           // 2 warps,  64 KB, 3/SM
 using C5 = Cfg<64, 128, 2, 2, 8, 3, kLoaderTma, 3>;          // 4 warps,  72 KB, 3/SM
 using C6 = Cfg<128, 64, 4, 1, 8, 3, kLoaderTma, 3>;          // 4 warps,  72 KB, 3/SM
-// Rolled core: 4 four-deep steps per loop iteration, double-buffered fragments.
-using R0 = Cfg<128, 256, 4, 2, 16, 4, kLoaderTma, 1, 4, 3>;
-using R1 = Cfg<128, 128, 4, 1, 16, 3, kLoaderTma, 2, 4, 3>;
-using R2 = Cfg<128, 64, 4, 1, 8, 3, kLoaderTma, 3, 4, 3>;
-using R3 = Cfg<64, 128, 2, 2, 8, 3, kLoaderTma, 3, 4, 3>;
+// Lane map 1 (a quarter-warp owns 4 rows x 2 column groups): same
+// arithmetic, ~0.5% faster than map 0 on this tile at 4096..16384.
+using M1 = Cfg<128, 64, 4, 1, 8, 3, kLoaderTma, 3, 8, 1>;
 using C8 = Cfg<128, 256, 4, 2, 16, 4, kLoaderAsync4, 1>;
 using C9 = Cfg<128, 128, 4, 2, 8, 3, kLoaderAsync4, 2>;
 using C11 = Cfg<64, 128, 2, 2, 8, 4, kLoaderAsync4, 2>;
 using C12 = Cfg<64, 64, 2, 1, 8, 4, kLoaderAsync4, 3>;
 using C14 = Cfg<128, 64, 4, 1, 8, 3, kLoaderAsync4, 3>;
-using R5 = Cfg<128, 128, 4, 1, 16, 3, kLoaderAsync4, 2, 4, 3>;
-using R6 = Cfg<128, 64, 4, 1, 8, 3, kLoaderAsync4, 3, 4, 3>;
 
 struct ConfigDesc {
     const char* name;
@@ -52,12 +48,10 @@ static const ConfigDesc kConfigs[] = {
     describe<C0>("tma_128x256_w8_t8x16_s4", 0.95f),    describe<C1>("tma_128x128_w8_t8x8_s3", 0.96f),
     describe<C2>("tma_128x128_w4_t8x16_s3", 0.95f),    describe<C3>("tma_64x128_w4_t8x8_s4", 0.96f),
     describe<C4>("tma_64x64_w2_t8x8_s4", 0.82f),       describe<C5>("tma_64x128_w4_t8x8_s3", 0.97f),
-    describe<C6>("tma_128x64_w4_t8x8_s3", 0.99f),      describe<R0>("tma_128x256_w8_t8x16_s4_r4", 0.99f),
-    describe<R1>("tma_128x128_w4_t8x16_s3_r4", 1.00f), describe<R2>("tma_128x64_w4_t8x8_s3_r4", 1.00f),
-    describe<R3>("tma_64x128_w4_t8x8_s3_r4", 0.99f),   describe<C8>("cpa_128x256_w8_t8x16_s4", 0.62f),
+    describe<C6>("tma_128x64_w4_t8x8_s3", 0.99f),      describe<M1>("tma_128x64_w4_t8x8_s3_m1", 1.00f),
+    describe<C8>("cpa_128x256_w8_t8x16_s4", 0.62f),
     describe<C9>("cpa_128x128_w8_t8x8_s3", 0.62f),     describe<C11>("cpa_64x128_w4_t8x8_s4", 0.55f),
     describe<C12>("cpa_64x64_w2_t8x8_s4", 0.43f),      describe<C14>("cpa_128x64_w4_t8x8_s3", 0.59f),
-    describe<R5>("cpa_128x128_w4_t8x16_s3_r4", 0.62f), describe<R6>("cpa_128x64_w4_t8x8_s3_r4", 0.62f),
 };
 constexpr int kNumConfigs = sizeof(kConfigs) / sizeof(kConfigs[0]);
 

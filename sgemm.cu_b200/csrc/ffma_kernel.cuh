@@ -35,15 +35,14 @@ namespace ffma {
 enum Loader { kLoaderTma = 0, kLoaderAsync4 = 1 };
 
 template <int BM_, int BN_, int WM_, int WN_, int TN_, int STAGES_, int LOADER_, int MINB_ = 1,
-          int K4U_ = 8, int PIPE_ = 0>
+          int K4U_ = 8, int MAP_ = 0>
 struct Cfg {
     static constexpr int BM = BM_, BN = BN_, WM = WM_, WN = WN_, TN = TN_, STAGES = STAGES_;
     static constexpr int LOADER = LOADER_;
     static constexpr int MINB = MINB_;  // resident CTAs per SM the register budget targets
     static constexpr int K4U = K4U_;    // unroll of the 8 four-deep k steps of a k block
-    // 0: fully unrolled, compiler-scheduled; 1: double-buffered LDS.128 fragments;
-    // 2: A via LDS.64; 3: rolled loop of K4U four-deep steps, double-buffered
-    static constexpr int PIPE = PIPE_;
+    // Lane map onto the warp's 4 (m) x 8 (n) lane grid; see lane_coords().
+    static constexpr int MAP = MAP_;
     static constexpr int BK = 32;  // one 128-byte row of A per k block
     static constexpr int TM = 8;
     static constexpr int THREADS = 32 * WM * WN;
@@ -57,6 +56,29 @@ struct Cfg {
     static constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024;  // + alignment slack
 };
 
+
+// Lane -> (lm, ln) on the 4 x 8 lane grid.  The map only decides which
+// thread owns which outputs (every output keeps its own k-ordered FMA chain),
+// but it sets how many shared-memory wavefronts each 128-bit fragment load
+// takes, because the hardware serves a 128-bit load by quarter-warps.
+//   0: lm = lane / 8, ln = lane % 8 -- a quarter-warp reads one A row
+//      (broadcast) and 128 contiguous bytes of B;
+//   1: lm = lane % 4, ln = lane / 4 -- a quarter-warp reads 4 A rows and
+//      2 B chunks;
+//   2: a quarter-warp is a 2 (m) x 4 (n) block: 2 A rows, 4 B chunks.
+template <int MAP>
+__device__ __forceinline__ void lane_coords(int lane, int& lm, int& ln) {
+    if constexpr (MAP == 1) {
+        lm = lane & 3;
+        ln = lane >> 2;
+    } else if constexpr (MAP == 2) {
+        lm = (lane & 1) | ((lane >> 3) & 2);
+        ln = ((lane >> 1) & 3) | ((lane >> 1) & 4);
+    } else {
+        lm = lane >> 3;
+        ln = lane & 7;
+    }
+}
 
 // Grouped rasterisation: 8 tile-rows share a band so concurrently resident
 // CTAs reuse A rows and B columns out of L2.
@@ -93,140 +115,11 @@ __device__ __forceinline__ void load_b_frag(const uint8_t* __restrict__ Bs, uint
         b[g] = *reinterpret_cast<const float4*>(Bs + k * C::BN * 4 + b_base + g * 128);
 }
 
-// Same arithmetic as compute_stage, with the next fragments loaded one step
-// ahead into a second register set (A one 4-deep step ahead, B one k ahead),
-// so shared-memory latency overlaps the current step's FFMAs.
+// Accumulate one 32-deep k block held in shared memory: A fragments for a
+// 4-deep step at its start, B per k (the compiler schedules the loads).  Each
+// element accumulates over k in increasing order with one FMA per term.
 template <class C>
-__device__ __forceinline__ void compute_stage_pipelined(const uint8_t* __restrict__ As,
-                                                        const uint8_t* __restrict__ Bs,
-                                                        uint32_t a_base, uint32_t xa0,
-                                                        uint32_t xa1, uint32_t b_base,
-                                                        float (&acc)[C::TM][C::TN]) {
-    float4 a[2][C::TM];
-    float4 b[2][C::TN / 4];
-    load_a_frag<C>(As, a_base, xa0, xa1, 0, a[0]);
-    load_b_frag<C>(Bs, b_base, 0, b[0]);
-#pragma unroll
-    for (int k4 = 0; k4 < C::BK / 4; ++k4) {
-#pragma unroll
-        for (int kk = 0; kk < 4; ++kk) {
-            const int k = 4 * k4 + kk;
-            if (kk == 0 && k4 + 1 < C::BK / 4)
-                load_a_frag<C>(As, a_base, xa0, xa1, k4 + 1, a[(k4 + 1) & 1]);
-            if (k + 1 < C::BK) load_b_frag<C>(Bs, b_base, k + 1, b[(k + 1) & 1]);
-            const float4(&ac)[C::TM] = a[k4 & 1];
-            const float4(&bc)[C::TN / 4] = b[k & 1];
-#pragma unroll
-            for (int i = 0; i < C::TM; ++i) {
-                const float av = kk == 0 ? ac[i].x : kk == 1 ? ac[i].y : kk == 2 ? ac[i].z : ac[i].w;
-#pragma unroll
-                for (int g = 0; g < C::TN / 4; ++g) {
-                    acc[i][4 * g + 0] = fmaf(av, bc[g].x, acc[i][4 * g + 0]);
-                    acc[i][4 * g + 1] = fmaf(av, bc[g].y, acc[i][4 * g + 1]);
-                    acc[i][4 * g + 2] = fmaf(av, bc[g].z, acc[i][4 * g + 2]);
-                    acc[i][4 * g + 3] = fmaf(av, bc[g].w, acc[i][4 * g + 3]);
-                }
-            }
-        }
-    }
-}
-
-// Variant for wide thread tiles (8 x 16): A is read two k-values at a time
-// (LDS.64), halving the registers its double buffer needs; B one k ahead.
-template <class C>
-__device__ __forceinline__ void compute_stage_pipelined64(const uint8_t* __restrict__ As,
-                                                          const uint8_t* __restrict__ Bs,
-                                                          uint32_t a_base, uint32_t xa0,
-                                                          uint32_t xa1, uint32_t b_base,
-                                                          float (&acc)[C::TM][C::TN]) {
-    float2 a[2][C::TM];
-    float4 b[2][C::TN / 4];
-    auto load_a2 = [&](int kp, float2 (&dst)[C::TM]) {
-#pragma unroll
-        for (int i = 0; i < C::TM; ++i) {
-            const uint32_t x = (i & 1) ? xa1 : xa0;
-            const uint32_t off = a_base + i * 4 * 128 +
-                                 ((static_cast<uint32_t>(kp >> 1) << 4) ^ x) + ((kp & 1) << 3);
-            dst[i] = *reinterpret_cast<const float2*>(As + off);
-        }
-    };
-    load_a2(0, a[0]);
-    load_b_frag<C>(Bs, b_base, 0, b[0]);
-#pragma unroll
-    for (int kp = 0; kp < C::BK / 2; ++kp) {
-#pragma unroll
-        for (int kk = 0; kk < 2; ++kk) {
-            const int k = 2 * kp + kk;
-            if (kk == 0 && kp + 1 < C::BK / 2) load_a2(kp + 1, a[(kp + 1) & 1]);
-            if (k + 1 < C::BK) load_b_frag<C>(Bs, b_base, k + 1, b[(k + 1) & 1]);
-            const float2(&ac)[C::TM] = a[kp & 1];
-            const float4(&bc)[C::TN / 4] = b[k & 1];
-#pragma unroll
-            for (int i = 0; i < C::TM; ++i) {
-                const float av = kk == 0 ? ac[i].x : ac[i].y;
-#pragma unroll
-                for (int g = 0; g < C::TN / 4; ++g) {
-                    acc[i][4 * g + 0] = fmaf(av, bc[g].x, acc[i][4 * g + 0]);
-                    acc[i][4 * g + 1] = fmaf(av, bc[g].y, acc[i][4 * g + 1]);
-                    acc[i][4 * g + 2] = fmaf(av, bc[g].z, acc[i][4 * g + 2]);
-                    acc[i][4 * g + 3] = fmaf(av, bc[g].w, acc[i][4 * g + 3]);
-                }
-            }
-        }
-    }
-}
-
-// Compact pipelined core: the 8 four-deep steps of a k block run as a rolled
-// loop of 8 / G iterations with G steps unrolled in each, so the loop body
-// (G x 4 x TM x TN FFMAs) stays small enough for the instruction cache; the
-// fragment double buffering continues across iterations, with the loads past
-// the end of the block predicated off.
-template <class C>
-__device__ __forceinline__ void compute_stage_rolled(const uint8_t* __restrict__ As,
-                                                     const uint8_t* __restrict__ Bs,
-                                                     uint32_t a_base, uint32_t xa0, uint32_t xa1,
-                                                     uint32_t b_base, float (&acc)[C::TM][C::TN]) {
-    constexpr int G = C::K4U;  // four-deep steps per loop iteration: even, so the
-    static_assert(G == 2 || G == 4, "");  // double-buffer slots stay compile-time
-    constexpr int NK4 = C::BK / 4;
-    float4 a[2][C::TM];
-    float4 b[2][C::TN / 4];
-    load_a_frag<C>(As, a_base, xa0, xa1, 0, a[0]);
-    load_b_frag<C>(Bs, b_base, 0, b[0]);
-#pragma unroll 1
-    for (int it = 0; it < NK4 / G; ++it) {
-#pragma unroll
-        for (int u = 0; u < G; ++u) {
-            const int k4 = it * G + u;
-#pragma unroll
-            for (int kk = 0; kk < 4; ++kk) {
-                const int k = 4 * k4 + kk;
-                const int bufa = u & 1;  // k4 & 1, since it * G is even
-                if (kk == 0 && k4 + 1 < NK4) load_a_frag<C>(As, a_base, xa0, xa1, k4 + 1, a[bufa ^ 1]);
-                if (k + 1 < C::BK) load_b_frag<C>(Bs, b_base, k + 1, b[(kk + 1) & 1]);
-                const float4(&ac)[C::TM] = a[bufa];
-                const float4(&bc)[C::TN / 4] = b[kk & 1];
-#pragma unroll
-                for (int i = 0; i < C::TM; ++i) {
-                    const float av =
-                        kk == 0 ? ac[i].x : kk == 1 ? ac[i].y : kk == 2 ? ac[i].z : ac[i].w;
-#pragma unroll
-                    for (int g = 0; g < C::TN / 4; ++g) {
-                        acc[i][4 * g + 0] = fmaf(av, bc[g].x, acc[i][4 * g + 0]);
-                        acc[i][4 * g + 1] = fmaf(av, bc[g].y, acc[i][4 * g + 1]);
-                        acc[i][4 * g + 2] = fmaf(av, bc[g].z, acc[i][4 * g + 2]);
-                        acc[i][4 * g + 3] = fmaf(av, bc[g].w, acc[i][4 * g + 3]);
-                    }
-                }
-            }
-        }
-    }
-}
-
-// Fragment-at-a-time core: A for a 4-deep step at its start, B per k (the
-// compiler schedules the loads).
-template <class C>
-__device__ __forceinline__ void compute_stage_simple(const uint8_t* __restrict__ As,
+__device__ __forceinline__ void compute_stage(const uint8_t* __restrict__ As,
                                                      const uint8_t* __restrict__ Bs,
                                                      uint32_t a_base, uint32_t xa0, uint32_t xa1,
                                                      uint32_t b_base, float (&acc)[C::TM][C::TN]) {
@@ -259,23 +152,6 @@ __device__ __forceinline__ void compute_stage_simple(const uint8_t* __restrict__
             }
         }
     }
-}
-
-// Accumulate one 32-deep k block held in shared memory.  Every variant
-// accumulates each element over k in increasing order with one FMA per term.
-template <class C>
-__device__ __forceinline__ void compute_stage(const uint8_t* __restrict__ As,
-                                              const uint8_t* __restrict__ Bs, uint32_t a_base,
-                                              uint32_t xa0, uint32_t xa1, uint32_t b_base,
-                                              float (&acc)[C::TM][C::TN]) {
-    if constexpr (C::PIPE == 1)
-        compute_stage_pipelined<C>(As, Bs, a_base, xa0, xa1, b_base, acc);
-    else if constexpr (C::PIPE == 3)
-        compute_stage_rolled<C>(As, Bs, a_base, xa0, xa1, b_base, acc);
-    else if constexpr (C::PIPE == 2)
-        compute_stage_pipelined64<C>(As, Bs, a_base, xa0, xa1, b_base, acc);
-    else
-        compute_stage_simple<C>(As, Bs, a_base, xa0, xa1, b_base, acc);
 }
 
 // Operand and output views of one GEMM, shared by the single-problem kernel
@@ -372,7 +248,8 @@ __global__ void __launch_bounds__(C::THREADS, C::MINB)
     const int tid = threadIdx.x;
     const int warp = tid >> 5, lane = tid & 31;
     const int wm = warp / C::WN, wn = warp % C::WN;
-    const int lm = lane >> 3, ln = lane & 7;
+    int lm, ln;
+    lane_coords<C::MAP>(lane, lm, ln);
 
     int tm, tn;
     tile_coords(blockIdx.x, p.tiles_m, p.tiles_n, tm, tn);

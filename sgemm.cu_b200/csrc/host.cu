@@ -1,0 +1,271 @@
+// host.cu — GEMM on operands that live in host memory.
+//
+// The reference has no such entry point: its callers copy A, B and C to the
+// device with cudaMemcpy, call sgemm(), and copy C back (test.cu:70-80,
+// benchmark.cu:69-73), so the PCIe transfers and the kernel run one after the
+// other.  Here the library stages the operands through HBM itself and overlaps
+// the three phases.  C is cut into blocks: row bands (at most 16, multiples of
+// 128 rows) times column chunks (1..4, multiples of 128 columns); the blocks
+// go column chunk by column chunk:
+//
+//   copy stream (H2D):  B[:, chunk j], then per row band b: A[b, :] (first
+//                       chunk only) and, when beta != 0, C[b, chunk j]
+//   compute streams:    block (b, j) runs on one of four compute streams as soon
+//                       as its operands have landed, so a block's kernel
+//                       overlaps its neighbours' copies and wave tails
+//   copy stream (D2H):  C[b, chunk j] back to the host once computed
+//
+// Column chunks let the first kernel start after 1/S of B instead of all of
+// it; the number of chunks comes from a small timing model of this pipeline
+// (PCIe bandwidth and per-path GEMM rate measured on a B200), evaluated for
+// 1..4 chunks per call.  Every block is the same GEMM on a sub-matrix, issued
+// through sgemm_b200_gemm(); each C element keeps its k-ordered accumulation,
+// so the result is bit-identical to copying the whole matrices and calling the
+// device entry point once.
+//
+// Device memory: A, B and C at 16-byte-aligned pitches, from the library's
+// stream-ordered pool.  Host buffers should be page-locked (cudaMallocHost /
+// cudaHostRegister): pageable memory gives the same result, but the driver
+// then stages copies synchronously and nothing overlaps.  Device pointers are
+// accepted too (the copies use cudaMemcpyDefault).
+#include <algorithm>
+#include <mutex>
+
+#include "common.h"
+
+namespace sgb {
+namespace host {
+
+constexpr int kComputeStreams = 4;
+constexpr int kMaxBands = 16;
+constexpr int kMaxChunks = 4;
+constexpr int kMaxBlocks = kMaxBands * kMaxChunks;
+
+struct Engine {
+    bool ready = false;
+    cudaStream_t h2d = nullptr, d2h = nullptr, comp[kComputeStreams] = {};
+    cudaEvent_t start = nullptr;
+    cudaEvent_t b_in[kMaxChunks] = {}, in[kMaxBlocks] = {}, done[kMaxBlocks] = {};
+    cudaEvent_t tail[2 + kComputeStreams] = {};
+    std::mutex mu;  // one call at a time enqueues on the engine's streams and events
+};
+
+static Engine* engine() {
+    constexpr int kMaxDevices = 64;
+    static Engine engines[kMaxDevices];
+    static std::mutex mu;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return nullptr;
+    std::lock_guard<std::mutex> lock(mu);
+    Engine& e = engines[dev];
+    if (!e.ready) {
+        const unsigned sf = cudaStreamNonBlocking;
+        const unsigned ef = cudaEventDisableTiming;
+        bool ok = cudaStreamCreateWithFlags(&e.h2d, sf) == cudaSuccess &&
+                  cudaStreamCreateWithFlags(&e.d2h, sf) == cudaSuccess &&
+                  cudaEventCreateWithFlags(&e.start, ef) == cudaSuccess;
+        for (int i = 0; ok && i < kComputeStreams; ++i)
+            ok = cudaStreamCreateWithFlags(&e.comp[i], sf) == cudaSuccess;
+        for (int i = 0; ok && i < kMaxChunks; ++i)
+            ok = cudaEventCreateWithFlags(&e.b_in[i], ef) == cudaSuccess;
+        for (int i = 0; ok && i < kMaxBlocks; ++i)
+            ok = cudaEventCreateWithFlags(&e.in[i], ef) == cudaSuccess &&
+                 cudaEventCreateWithFlags(&e.done[i], ef) == cudaSuccess;
+        for (int i = 0; ok && i < 2 + kComputeStreams; ++i)
+            ok = cudaEventCreateWithFlags(&e.tail[i], ef) == cudaSuccess;
+        if (!ok) return nullptr;  // partially created handles live until exit
+        e.ready = true;
+    }
+    return &e;
+}
+
+static size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+// Smallest block worth a kernel of its own: one 128 x 64 CTA tile per SM.
+// With four compute streams, four such blocks in flight cover every resident
+// CTA slot, so the timing model's "GEMMs run at full rate" stays true.
+constexpr double kMinBlockElems = 148.0 * 128 * 64;
+
+// Rows per band for blocks `cols` wide: at most kMaxBands bands, blocks of at
+// least kMinBlockElems, a multiple of 128 rows (the tallest CTA tile), and
+// bands of even height.
+static int band_rows(int m, int cols) {
+    const int r_min = static_cast<int>((kMinBlockElems + cols - 1) / cols);
+    int r = std::max((m + kMaxBands - 1) / kMaxBands, r_min);
+    r = (r + 127) / 128 * 128;
+    if (r >= m) return m;
+    const int bands = (m + r - 1) / r;
+    r = ((m + bands - 1) / bands + 127) / 128 * 128;
+    return std::min(m, r);
+}
+
+// Columns per chunk for `chunks` chunks: a multiple of 128, the last chunk
+// takes the rest.
+static int chunk_cols(int n, int chunks) {
+    if (chunks <= 1) return n;
+    const int c = (n + chunks - 1) / chunks;
+    return std::min(n, (c + 127) / 128 * 128);
+}
+
+// Timing model of the pipeline: one H2D queue, one D2H queue, and the GEMMs
+// as one server at the path's rate.  Constants measured on a B200 (pinned
+// host memory; GEMM rates at 8192^3).
+static double model_ms(int path, int m, int n, int k, bool read_c, int rows, int cols) {
+    constexpr double kPcieBytesPerS = 51e9;
+    const double flops_per_s = path == SGEMM_B200_PATH_BF16X6   ? 245e12
+                               : path == SGEMM_B200_PATH_TF32X3 ? 230e12
+                                                                : 54e12;
+    double t_h = 0, t_c = 0, t_d = 0;
+    for (int c0 = 0; c0 < n; c0 += cols) {
+        const double nc = std::min(cols, n - c0);
+        t_h += 4.0 * k * nc / kPcieBytesPerS;
+        for (int r0 = 0; r0 < m; r0 += rows) {
+            const double nr = std::min(rows, m - r0);
+            if (c0 == 0) t_h += 4.0 * nr * k / kPcieBytesPerS;
+            if (read_c) t_h += 4.0 * nr * nc / kPcieBytesPerS;
+            t_c = std::max(t_c, t_h) + 2.0 * nr * nc * k / flops_per_s;
+            t_d = std::max(t_d, t_c) + 4.0 * nr * nc / kPcieBytesPerS;
+        }
+    }
+    return t_d * 1e3;
+}
+
+struct Plan {
+    int rows, cols;
+};
+
+Plan make_plan(int path, int m, int n, int k, bool read_c) {
+    const double bytes = 4.0 * (double(m) * k + double(k) * n + double(m) * n * (read_c ? 2 : 1));
+    if (bytes < 16.0 * (1 << 20)) return Plan{m, n};  // small: one block
+    Plan p{band_rows(m, n), n};
+    double best = model_ms(path, m, n, k, read_c, p.rows, n);
+    for (int s = 2; s <= kMaxChunks; ++s) {
+        const int cols = chunk_cols(n, s);
+        if (cols < 512 || cols >= n) break;
+        const int rows = band_rows(m, cols);
+        const double t = model_ms(path, m, n, k, read_c, rows, cols);
+        if (t < best * 0.98) {  // fewer, larger blocks unless clearly slower
+            best = t;
+            p = Plan{rows, cols};
+        }
+    }
+    return p;
+}
+
+static int run(int path, int m, int n, int k, const float* alpha, const float* A, int lda,
+               const float* B, int ldb, const float* beta, float* C, int ldc,
+               cudaStream_t stream) {
+    Engine* eng = engine();
+    if (!eng) return SGEMM_B200_ERR_CUDA;
+    cudaMemPool_t pool = library_pool();
+    if (!pool) return SGEMM_B200_ERR_CUDA;
+
+    const bool read_c = *beta != 0.0f;  // beta == 0: C is written, never read
+    const Plan plan = make_plan(path, m, n, k, read_c);
+    const int bands = (m + plan.rows - 1) / plan.rows;
+    const int chunks = (n + plan.cols - 1) / plan.cols;
+    // Device pitches: rows start on 16 bytes, so the TMA kernels take every block.
+    const int lda_d = (k + 3) / 4 * 4, ldb_d = (n + 3) / 4 * 4, ldc_d = (n + 3) / 4 * 4;
+    const size_t a_bytes = align_up(sizeof(float) * (size_t)m * lda_d, 256);
+    const size_t b_bytes = align_up(sizeof(float) * (size_t)k * ldb_d, 256);
+    const size_t c_bytes = align_up(sizeof(float) * (size_t)m * ldc_d, 256);
+
+    std::lock_guard<std::mutex> lock(eng->mu);
+    void* base = nullptr;
+    cudaError_t e = cudaMallocFromPoolAsync(&base, a_bytes + b_bytes + c_bytes, pool, stream);
+    if (e != cudaSuccess) return cuda_status(e);
+    float* dA = static_cast<float*>(base);
+    float* dB = reinterpret_cast<float*>(static_cast<char*>(base) + a_bytes);
+    float* dC = reinterpret_cast<float*>(static_cast<char*>(base) + a_bytes + b_bytes);
+
+    int status = SGEMM_B200_OK;
+    auto ok = [&](cudaError_t r) {
+        if (r != cudaSuccess && status == SGEMM_B200_OK) status = cuda_status(r);
+        return status == SGEMM_B200_OK;
+    };
+    const size_t f = sizeof(float);
+    cudaStream_t all[2 + kComputeStreams];
+    all[0] = eng->h2d;
+    all[1] = eng->d2h;
+    for (int i = 0; i < kComputeStreams; ++i) all[2 + i] = eng->comp[i];
+    // Everything below starts after the caller's prior work and the allocation.
+    if (ok(cudaEventRecord(eng->start, stream)))
+        for (cudaStream_t s : all) ok(cudaStreamWaitEvent(s, eng->start, 0));
+
+    int blk = 0;
+    for (int j = 0; j < chunks && status == SGEMM_B200_OK; ++j) {
+        const int c0 = j * plan.cols, nc = std::min(plan.cols, n - c0);
+        if (k > 0 && ok(cudaMemcpy2DAsync(dB + c0, f * ldb_d, B + c0, f * ldb, f * nc, k,
+                                          cudaMemcpyDefault, eng->h2d)))
+            ok(cudaEventRecord(eng->b_in[j], eng->h2d));
+        for (int b = 0; b < bands && status == SGEMM_B200_OK; ++b, ++blk) {
+            const int r0 = b * plan.rows, nr = std::min(plan.rows, m - r0);
+            cudaStream_t cs = eng->comp[blk % kComputeStreams];
+            // H2D: this block's operands (A's band only with the first chunk).
+            if (j == 0 && k > 0 &&
+                !ok(cudaMemcpy2DAsync(dA + (size_t)r0 * lda_d, f * lda_d, A + (size_t)r0 * lda,
+                                      f * lda, f * k, nr, cudaMemcpyDefault, eng->h2d)))
+                break;
+            if (read_c &&
+                !ok(cudaMemcpy2DAsync(dC + (size_t)r0 * ldc_d + c0, f * ldc_d,
+                                      C + (size_t)r0 * ldc + c0, f * ldc, f * nc, nr,
+                                      cudaMemcpyDefault, eng->h2d)))
+                break;
+            if (!ok(cudaEventRecord(eng->in[blk], eng->h2d))) break;
+            // Compute.
+            if (k > 0 && !ok(cudaStreamWaitEvent(cs, eng->b_in[j], 0))) break;
+            if (!ok(cudaStreamWaitEvent(cs, eng->in[blk], 0))) break;
+            const int g = sgemm_b200_gemm(path, nr, nc, k, alpha, dA + (size_t)r0 * lda_d, lda_d,
+                                          dB + c0, ldb_d, beta, dC + (size_t)r0 * ldc_d + c0,
+                                          ldc_d, reinterpret_cast<sgemm_b200_stream_t>(cs));
+            if (g != SGEMM_B200_OK) {
+                status = g;
+                break;
+            }
+            if (!ok(cudaEventRecord(eng->done[blk], cs))) break;
+            // D2H.
+            if (ok(cudaStreamWaitEvent(eng->d2h, eng->done[blk], 0)))
+                ok(cudaMemcpy2DAsync(C + (size_t)r0 * ldc + c0, f * ldc,
+                                     dC + (size_t)r0 * ldc_d + c0, f * ldc_d, f * nc, nr,
+                                     cudaMemcpyDefault, eng->d2h));
+        }
+    }
+    // Join: the caller's stream waits for whatever was enqueued on the
+    // engine's streams (also after an error), then releases the staging memory.
+    for (int i = 0; i < 2 + kComputeStreams; ++i) {
+        if (cudaEventRecord(eng->tail[i], all[i]) == cudaSuccess)
+            cudaStreamWaitEvent(stream, eng->tail[i], 0);
+    }
+    cudaFreeAsync(base, stream);
+    return status;
+}
+
+}  // namespace host
+}  // namespace sgb
+
+extern "C" int sgemm_b200_host(int path, int m, int n, int k, const float* alpha, const float* A,
+                               int lda, const float* B, int ldb, const float* beta, float* C,
+                               int ldc, sgemm_b200_stream_t stream) {
+    int s = sgb::check_gemm_args(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+    if (s == SGEMM_B200_OK && path != SGEMM_B200_PATH_PLAIN && path != SGEMM_B200_PATH_BF16X6 &&
+        path != SGEMM_B200_PATH_TF32X3)
+        s = SGEMM_B200_ERR_INVALID_ARG;
+    if (s == SGEMM_B200_OK && m > 0 && n > 0) {
+        if (!sgb::device_is_sm100())
+            s = SGEMM_B200_ERR_UNSUPPORTED;
+        else
+            s = sgb::host::run(path, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc,
+                               sgb::as_stream(stream));
+    }
+    sgb::set_last_status(s);
+    return s;
+}
+
+extern "C" int sgemm_b200_host_plan(int path, int m, int n, int k, int reads_c, int* rows,
+                                    int* cols) {
+    if (m <= 0 || n <= 0 || k < 0 || !rows || !cols) return SGEMM_B200_ERR_INVALID_ARG;
+    const sgb::host::Plan p = sgb::host::make_plan(path, m, n, k, reads_c != 0);
+    *rows = p.rows;
+    *cols = p.cols;
+    return SGEMM_B200_OK;
+}

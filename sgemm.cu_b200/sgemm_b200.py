@@ -104,6 +104,8 @@ def _declare(lib: ctypes.CDLL) -> None:
     d("sgemm_b200_split_workspace_size", ctypes.c_size_t, [_I, _I, _I, _I])
     d("sgemm_b200_split", _I, [_I] + _GEMM_ARGS + [_P, ctypes.c_size_t, _P])
     d("sgemm_b200_gemm", _I, [_I] + _GEMM_ARGS + [_P])
+    d("sgemm_b200_host", _I, [_I] + _GEMM_ARGS + [_P])
+    d("sgemm_b200_host_plan", _I, [_I, _I, _I, _I, _I, ctypes.POINTER(_I), ctypes.POINTER(_I)])
     d("sgemm_b200_grouped_plan_create", _I,
       [ctypes.POINTER(_P), ctypes.POINTER(Problem), _I, ctypes.c_char_p])
     d("sgemm_b200_grouped_plan_launch", _I, [_P, _P, _I])
@@ -182,12 +184,12 @@ def _stream_ptr(stream) -> Optional[int]:
     return stream.cuda_stream  # torch.cuda.Stream
 
 
-def _mat(t, name: str):
-    """(device pointer, row stride) of a 2-D row-major float32 CUDA tensor."""
+def _mat(t, name: str, device: str = "cuda"):
+    """(pointer, row stride) of a 2-D row-major float32 tensor on `device`."""
     import torch
 
-    if t.dtype != torch.float32 or t.dim() != 2 or not t.is_cuda:
-        raise ValueError(f"{name} must be a 2-D float32 CUDA tensor")
+    if t.dtype != torch.float32 or t.dim() != 2 or t.device.type != device:
+        raise ValueError(f"{name} must be a 2-D float32 {device.upper()} tensor")
     if t.stride(1) != 1:
         raise ValueError(f"{name} must be row-major with unit column stride")
     ld = t.stride(0) if t.size(0) > 1 else max(t.size(1), 1)
@@ -247,6 +249,32 @@ def gemm(path, A, B, C, alpha: float = 1.0, beta: float = 0.0, stream=None) -> N
     pc, ldc = _mat(C, "C")
     _check(lib().sgemm_b200_gemm(p, m, n, k, _f(alpha), pa, lda, pb, ldb, _f(beta), pc, ldc,
                                  _stream_ptr(stream)), "sgemm_b200_gemm")
+
+
+def sgemm_host(A, B, C, alpha: float = 1.0, beta: float = 0.0, path="plain",
+               stream=None) -> None:
+    """C := alpha*A@B + beta*C with A, B, C in HOST memory (CPU tensors, ideally
+    pinned): the library stages blocks of C through HBM with the copies
+    overlapping the kernels, and writes C back in place."""
+    p = PATHS[path] if isinstance(path, str) else int(path)
+    m, k = A.shape
+    k2, n = B.shape
+    if k2 != k or tuple(C.shape) != (m, n):
+        raise ValueError("shape mismatch")
+    pa, lda = _mat(A, "A", "cpu")
+    pb, ldb = _mat(B, "B", "cpu")
+    pc, ldc = _mat(C, "C", "cpu")
+    _check(lib().sgemm_b200_host(p, m, n, k, _f(alpha), pa, lda, pb, ldb, _f(beta), pc, ldc,
+                                 _stream_ptr(stream)), "sgemm_b200_host")
+
+
+def host_plan(m: int, n: int, k: int, reads_c: bool = True, path="plain") -> tuple:
+    """(rows per band, columns per chunk) sgemm_host uses for this problem."""
+    p = PATHS[path] if isinstance(path, str) else int(path)
+    r, c = ctypes.c_int(0), ctypes.c_int(0)
+    _check(lib().sgemm_b200_host_plan(p, m, n, k, int(reads_c), ctypes.byref(r), ctypes.byref(c)),
+           "sgemm_b200_host_plan")
+    return r.value, c.value
 
 
 def fill_random(X, seed: int, tag: int, dist: int = DIST_UNIFORM_PM1, stream=None) -> None:

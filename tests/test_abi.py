@@ -89,3 +89,28 @@ def test_config_table():
     assert names[c].startswith("cpa_")
     c = sg.lib().sgemm_b200_select_config(8192, 8192, 8192, 16, 8192, 16, 8192, 16, 8192)
     assert names[c].startswith("tma_")
+
+
+def test_host_entry_validation_and_bands():
+    l = sg.lib()
+    a = ctypes.c_float(1.0)
+    b = ctypes.c_float(0.5)
+    # argument checks run before any device work
+    assert l.sgemm_b200_host(0, 4, 4, 4, ctypes.byref(a), 16, 3, 16, 4, ctypes.byref(b), 16, 4,
+                             None) == sg.ERR_INVALID_ARG
+    assert l.sgemm_b200_host(9, 4, 4, 4, ctypes.byref(a), 16, 4, 16, 4, ctypes.byref(b), 16, 4,
+                             None) == sg.ERR_INVALID_ARG
+    assert l.sgemm_b200_host(0, 0, 4, 4, ctypes.byref(a), None, 4, None, 4, ctypes.byref(b),
+                             None, 4, None) == sg.OK
+    # blocking: <= 16 row bands of a multiple of 128 rows, <= 4 column chunks
+    # of a multiple of 128 columns; small problems in one block
+    assert sg.host_plan(8192, 8192, 8192) == (512, 4096)  # the model's pick
+    assert sg.host_plan(4096, 4096, 4096) == (384, 4096)
+    assert sg.host_plan(200, 8192, 8192)[0] == 200  # one band; B may still be chunked
+    assert sg.host_plan(1000, 1000, 1000) == (1000, 1000)  # < 16 MB moved
+    for m, n in ((3001, 4096), (5003, 5003), (8191, 777), (100000, 4096), (16384, 16384)):
+        for path in ("plain", "bf16x6", "tf32x3"):
+            r, c = sg.host_plan(m, n, 4096, True, path)
+            assert (r % 128 == 0 and 128 <= r <= m) or r == m
+            assert -(-m // r) <= 16
+            assert c == n or (c % 128 == 0 and c >= 512 and -(-n // c) <= 4)
