@@ -20,9 +20,6 @@ using C3 = Cfg<64, 128, 2, 2, 8, 4, kLoaderTma, 2>;          // 4 warps,  96 KB,
 using C4 = Cfg<64, 64, 2, 1, 8, 4, kLoaderTma, 3>;           // 2 warps,  64 KB, 3/SM
 using C5 = Cfg<64, 128, 2, 2, 8, 3, kLoaderTma, 3>;          // 4 warps,  72 KB, 3/SM
 using C6 = Cfg<128, 64, 4, 1, 8, 3, kLoaderTma, 3>;          // 4 warps,  72 KB, 3/SM
-// Lane map 1 (a quarter-warp owns 4 rows x 2 column groups): same
-// arithmetic, ~0.5% faster than map 0 on this tile at 4096..16384.
-using M1 = Cfg<128, 64, 4, 1, 8, 3, kLoaderTma, 3, 8, 1>;
 using C8 = Cfg<128, 256, 4, 2, 16, 4, kLoaderAsync4, 1>;
 using C9 = Cfg<128, 128, 4, 2, 8, 3, kLoaderAsync4, 2>;
 using C11 = Cfg<64, 128, 2, 2, 8, 4, kLoaderAsync4, 2>;
@@ -42,16 +39,20 @@ constexpr ConfigDesc describe(const char* name, float eff) {
                       &ffma_gemm_kernel<C>};
 }
 
-// Efficiencies: GFLOP/s measured on a B200 at 8192^3 (alpha=1.5, beta=0.5),
-// normalised to the best configuration of the same loader.
+// Efficiencies: GFLOP/s measured on a B200 at 8192^3 and 16384^3
+// (alpha=1.5, beta=0.5), normalised to the best configuration of the same
+// loader (TMA: tma_128x64_w4_t8x8_s3 at 54.97 / 55.77 TFLOP/s; cp.async:
+// cpa_128x256_w8_t8x16_s4 at 8191^3).  The two 8 x 16-thread TMA tiles are
+// rated at 4096^3, where their longer fill and drain costs them most (0.84 and
+// 0.875 there, 0.93 and 0.955 at 8192^3); above 3072 the 128 x 64 tile wins
+// whatever their rating.
 static const ConfigDesc kConfigs[] = {
-    describe<C0>("tma_128x256_w8_t8x16_s4", 0.95f),    describe<C1>("tma_128x128_w8_t8x8_s3", 0.96f),
-    describe<C2>("tma_128x128_w4_t8x16_s3", 0.95f),    describe<C3>("tma_64x128_w4_t8x8_s4", 0.96f),
-    describe<C4>("tma_64x64_w2_t8x8_s4", 0.82f),       describe<C5>("tma_64x128_w4_t8x8_s3", 0.97f),
-    describe<C6>("tma_128x64_w4_t8x8_s3", 0.99f),      describe<M1>("tma_128x64_w4_t8x8_s3_m1", 1.00f),
-    describe<C8>("cpa_128x256_w8_t8x16_s4", 0.62f),
-    describe<C9>("cpa_128x128_w8_t8x8_s3", 0.62f),     describe<C11>("cpa_64x128_w4_t8x8_s4", 0.55f),
-    describe<C12>("cpa_64x64_w2_t8x8_s4", 0.43f),      describe<C14>("cpa_128x64_w4_t8x8_s3", 0.59f),
+    describe<C0>("tma_128x256_w8_t8x16_s4", 0.840f),   describe<C1>("tma_128x128_w8_t8x8_s3", 0.925f),
+    describe<C2>("tma_128x128_w4_t8x16_s3", 0.875f),   describe<C3>("tma_64x128_w4_t8x8_s4", 0.952f),
+    describe<C4>("tma_64x64_w2_t8x8_s4", 0.815f),      describe<C5>("tma_64x128_w4_t8x8_s3", 0.994f),
+    describe<C6>("tma_128x64_w4_t8x8_s3", 1.000f),     describe<C8>("cpa_128x256_w8_t8x16_s4", 1.000f),
+    describe<C9>("cpa_128x128_w8_t8x8_s3", 0.920f),    describe<C11>("cpa_64x128_w4_t8x8_s4", 0.810f),
+    describe<C12>("cpa_64x64_w2_t8x8_s4", 0.630f),     describe<C14>("cpa_128x64_w4_t8x8_s3", 0.890f),
 };
 constexpr int kNumConfigs = sizeof(kConfigs) / sizeof(kConfigs[0]);
 
@@ -94,10 +95,20 @@ int plain_config_tile(int cfg, int* bm, int* bn) {
     return SGEMM_B200_OK;
 }
 
-// Pick the configuration with the smallest modelled time:
-//   waves(cfg) * tile_work(cfg) * resident(cfg) / efficiency(cfg)
-// where waves = ceil(tiles / (SMs * resident CTAs per SM)): the resident
-// CTAs of one wave share an SM, so each takes `resident` times as long.
+// Pick the configuration with the smallest modelled time.  A configuration
+// with `occ` resident CTAs per SM runs tiles in waves of SMs x occ; one CTA of
+// a full wave takes t = occ * BM * BN / efficiency (per-SM throughput shared
+// by occ CTAs).  The last, partial wave leaves r = ceil(remainder / SMs) < occ
+// CTAs on the busiest SM, which then runs at a fraction e(r) of its full
+// throughput (fewer warps to hide latency), so that wave takes
+// t * (r / occ) / e(r).  e(1) = 0.55 and e(2) = 0.85 (of 3) were fitted to
+// B200 sweeps of 768..4096 cubes, where the tile counts leave partial waves.
+static double partial_wave_cost(int r, int occ) {
+    if (r >= occ) return 1.0;
+    const double e = r == 1 ? 0.55 : 0.85;
+    return (double(r) / occ) / e;
+}
+
 int plain_select(int m, int n, int k, const float* A, int lda, const float* B, int ldb) {
     using namespace ffma;
     const int loader = (k == 0 || tma_ok(A, lda, B, ldb)) ? kLoaderTma : kLoaderAsync4;
@@ -108,10 +119,14 @@ int plain_select(int m, int n, int k, const float* A, int lda, const float* B, i
     for (int c = 0; c < kNumConfigs; ++c) {
         const ConfigDesc& cd = kConfigs[c];
         if (cd.loader != loader) continue;
+        const int occ = occupancy(c);
         const double tiles = double(div_up(m, cd.bm)) * div_up(n, cd.bn);
-        const double slots = double(sms) * occupancy(c);
-        const double waves = std::ceil(tiles / slots);
-        const double t = waves * double(cd.bm) * cd.bn * occupancy(c) / cd.efficiency;
+        const double slots = double(sms) * occ;
+        const double full = std::floor(tiles / slots);
+        const double rem = tiles - full * slots;
+        double waves = full;
+        if (rem > 0) waves += partial_wave_cost(static_cast<int>(std::ceil(rem / sms)), occ);
+        const double t = waves * occ * double(cd.bm) * cd.bn / cd.efficiency;
         if (best < 0 || t < best_t * 0.999) {
             best_t = t;
             best = c;

@@ -97,7 +97,8 @@ __device__ __forceinline__ bool run_item(const GParams& gp, const GProblem& pr, 
     const int tid = threadIdx.x;
     const int warp = tid >> 5, lane = tid & 31;
     const int wm = warp / C::WN, wn = warp % C::WN;
-    const int lm = lane >> 3, ln = lane & 7;
+    int lm, ln;
+    ffma::lane_coords(lane, lm, ln);
     const int m0 = it.tm * C::BM, n0 = it.tn * C::BN;
     const int nk = (pr.op.k + C::BK - 1) / C::BK;
     const int kb0 = it.ks * pr.kbps;
