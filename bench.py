@@ -256,8 +256,10 @@ def _cpu_baseline_and_parity(torch, sg, C_after, C0_host, size, target_s=10.0):
     hA = oracle.fill(size, size, SEED, 1, 0)
     hB = oracle.fill(size, size, SEED, 2, 0)
     threads = oracle.max_threads()
-    # calibrate on 32 rows, then take about target_s seconds of evenly spaced rows
+    # calibrate on 32 rows (after a warm-up that starts the OpenMP team and
+    # touches the operands), then take about target_s seconds of evenly spaced rows
     cal = np.linspace(0, size - 1, 32).astype(np.int32)
+    oracle.sgemm_basic_rows(cal[:8], hA, hB, C0_host[cal[:8]], ALPHA, BETA, basic=False)
     t0 = time.perf_counter()
     oracle.sgemm_basic_rows(cal, hA, hB, C0_host[cal], ALPHA, BETA, basic=False)
     per_row = (time.perf_counter() - t0) / len(cal)
