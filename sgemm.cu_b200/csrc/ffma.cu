@@ -39,13 +39,14 @@ constexpr ConfigDesc describe(const char* name, float eff) {
                       &ffma_gemm_kernel<C>};
 }
 
-// Efficiencies: GFLOP/s measured on a B200 at 8192^3 and 16384^3
-// (alpha=1.5, beta=0.5), normalised to the best configuration of the same
-// loader (TMA: tma_128x64_w4_t8x8_s3 at 54.97 / 55.77 TFLOP/s; cp.async:
-// cpa_128x256_w8_t8x16_s4 at 8191^3).  The two 8 x 16-thread TMA tiles are
-// rated at 4096^3, where their longer fill and drain costs them most (0.84 and
-// 0.875 there, 0.93 and 0.955 at 8192^3); above 3072 the 128 x 64 tile wins
-// whatever their rating.
+// Efficiencies: relative per-SM throughput of a full wave, normalised to the
+// best configuration of the same loader (TMA: tma_128x64_w4_t8x8_s3;
+// cp.async: cpa_128x256_w8_t8x16_s4).  First measured at 8192^3 / 16384^3
+// (the 8 x 16-thread tiles at 4096^3, where their longer fill and drain costs
+// them most), then checked against a B200 sweep of 256..16384 cubes with the
+// packed-FMA kernels: with plain_select's wave model the pick is within 2.1%
+// of the fastest configuration at every size and 0.2% on average, and a grid
+// refit of these numbers does no better.
 static const ConfigDesc kConfigs[] = {
     describe<C0>("tma_128x256_w8_t8x16_s4", 0.840f),   describe<C1>("tma_128x128_w8_t8x8_s3", 0.925f),
     describe<C2>("tma_128x128_w4_t8x16_s3", 0.875f),   describe<C3>("tma_64x128_w4_t8x8_s4", 0.952f),

@@ -21,6 +21,8 @@
 //  - B is kept [32][BN]; each 128-bit load is broadcast to the 4 lanes that
 //    share a column group (warp-level operand broadcast);
 //  - thread tile 8 (m) x TN (n); lanes 4 (m) x 8 (n); warps WM x WN;
+//  - the FMAs are packed (fma.rn.f32x2, two columns of a row per
+//    instruction): the FP32 pipe, not instruction issue, becomes the limit;
 //  - epilogue straight from registers with float4 stores: for a fixed
 //    register group a warp writes 4 rows x 128 contiguous bytes.
 #pragma once
@@ -127,10 +129,15 @@ __device__ __forceinline__ void compute_stage(const uint8_t* __restrict__ As,
             for (int g = 0; g < C::TN / 4; ++g)
                 b[g] = *reinterpret_cast<const float4*>(Bs + (k4 * 4 + kk) * C::BN * 4 + b_base +
                                                         g * 128);
-            // Outer product in serpentine order (row i left to right, row
-            // i+1 right to left), so consecutive FFMAs share an operand at
-            // every turn.  Measured on a B200: ~0.7% faster than row-major
-            // order, 4% faster than column-major order.
+            // Outer product with packed FP32 FMAs (fma.rn.f32x2): each
+            // instruction updates two neighbouring columns of one row,
+            // {c[i][j], c[i][j+1]} += {a_i, a_i} * {b_j, b_j+1}, with one
+            // round-to-nearest FMA per element -- the same arithmetic as two
+            // fmaf calls, in half the issue slots.  Rows run in serpentine
+            // order (row i left to right, row i+1 right to left) so
+            // consecutive instructions share an operand at every turn.
+            // Measured on a B200: +7.5% at 8192^3 over scalar FFMA; serpentine
+            // +0.7% over row-major with scalar FFMA.
             float av[C::TM], bv[C::TN];
 #pragma unroll
             for (int i = 0; i < C::TM; ++i)
@@ -143,12 +150,17 @@ __device__ __forceinline__ void compute_stage(const uint8_t* __restrict__ As,
                 bv[4 * g + 3] = b[g].w;
             }
 #pragma unroll
-            for (int i = 0; i < C::TM; ++i)
+            for (int i = 0; i < C::TM; ++i) {
+                const float2 a2 = make_float2(av[i], av[i]);
 #pragma unroll
-                for (int jj = 0; jj < C::TN; ++jj) {
-                    const int j = (i & 1) ? C::TN - 1 - jj : jj;
-                    acc[i][j] = fmaf(av[i], bv[j], acc[i][j]);
+                for (int pp = 0; pp < C::TN / 2; ++pp) {
+                    const int q = (i & 1) ? C::TN / 2 - 1 - pp : pp;
+                    float2 c = make_float2(acc[i][2 * q], acc[i][2 * q + 1]);
+                    c = __ffma2_rn(a2, make_float2(bv[2 * q], bv[2 * q + 1]), c);
+                    acc[i][2 * q] = c.x;
+                    acc[i][2 * q + 1] = c.y;
                 }
+            }
         }
     }
 }
