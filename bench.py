@@ -8,8 +8,10 @@ Inputs are 768 MB, larger than the 126 MB L2, and each timed step is bracketed
 by its own CUDA events with an L2-sized flush write in between steps.
 
   value        device-timed GFLOP/s, operands resident in HBM (max over ranks)
-  e2e          the same GEMM through the C ABI from pinned HOST buffers: H2D of
-               A, B, C, the GEMM, D2H of C -- all inside the timed region
+  e2e          the same GEMM through the C ABI from pinned HOST buffers
+               (sgemm_b200_host): H2D of A, B, C, the GEMM, D2H of C -- all
+               inside the timed region, the copies overlapped with block GEMMs;
+               the plain copy -> sgemm() -> copy sequence is reported beside it
   roofline     FP32 SIMT peak = SMs x 128 FMA lanes x 2 x SM clock
   cpu_baseline the oracle (C restatement of the reference's kernel_basic,
                OpenMP on the host cores) on a bounded sample of rows of the same
@@ -255,11 +257,13 @@ def _cpu_baseline_and_parity(torch, sg, C_after, C0_host, size, target_s=10.0):
     import oracle
     hA = oracle.fill(size, size, SEED, 1, 0)
     hB = oracle.fill(size, size, SEED, 2, 0)
+    # calibrate on 16 rows per host thread (after a warm-up that starts the
+    # OpenMP team and touches the operands), then take about target_s seconds
+    # of evenly spaced rows -- the whole matrix when it fits
     threads = oracle.max_threads()
-    # calibrate on 32 rows (after a warm-up that starts the OpenMP team and
-    # touches the operands), then take about target_s seconds of evenly spaced rows
-    cal = np.linspace(0, size - 1, 32).astype(np.int32)
-    oracle.sgemm_basic_rows(cal[:8], hA, hB, C0_host[cal[:8]], ALPHA, BETA, basic=False)
+    cal = np.linspace(0, size - 1, min(size, 16 * threads)).astype(np.int32)
+    oracle.sgemm_basic_rows(cal[:threads], hA, hB, C0_host[cal[:threads]], ALPHA, BETA,
+                            basic=False)
     t0 = time.perf_counter()
     oracle.sgemm_basic_rows(cal, hA, hB, C0_host[cal], ALPHA, BETA, basic=False)
     per_row = (time.perf_counter() - t0) / len(cal)

@@ -112,9 +112,9 @@ static int chunk_cols(int n, int chunks) {
 // host memory; GEMM rates at 8192^3).
 static double model_ms(int path, int m, int n, int k, bool read_c, int rows, int cols) {
     constexpr double kPcieBytesPerS = 51e9;
-    const double flops_per_s = path == SGEMM_B200_PATH_BF16X6   ? 245e12
-                               : path == SGEMM_B200_PATH_TF32X3 ? 230e12
-                                                                : 54e12;
+    const double flops_per_s = path == SGEMM_B200_PATH_BF16X6   ? 225e12
+                               : path == SGEMM_B200_PATH_TF32X3 ? 210e12
+                                                                : 59e12;
     double t_h = 0, t_c = 0, t_d = 0;
     for (int c0 = 0; c0 < n; c0 += cols) {
         const double nc = std::min(cols, n - c0);
