@@ -353,7 +353,7 @@ def _grouped_workload(n, seed):
     return [tuple(int(max(8, round(v / 8) * 8)) for v in row) for row in vals]
 
 
-def _grouped_leg(torch, sg, sms, sm_mhz):
+def _grouped_leg(torch, sg, sms, sm_mhz, hbm_gbs):
     """One persistent graph-captured launch over 512 uneven problems vs 512
     sequential plain launches; then the autotuned plan."""
     shapes = _grouped_workload(512, 7)
@@ -400,6 +400,11 @@ def _grouped_leg(torch, sg, sms, sm_mhz):
     os.unlink(tuned)
     peak = sms * 256 * sm_mhz * 1e-3  # GFLOP/s
     best = min(t_grouped, t_tuned)
+    # Roofline of the mix: each problem bounded by the SIMT peak or by HBM
+    # (4*(mk + kn + 2mn) bytes with beta != 0), summed over problems.
+    roof_ms = sum(max(2.0 * m * n * k / (peak * 1e9),
+                      4.0 * (m * k + k * n + 2 * m * n) / (hbm_gbs * 1e9))
+                  for m, n, k in shapes) * 1e3
     return {
         "workload": "512 problems, M,N,K log-uniform [64,4096] multiples of 8, alpha=1.5 "
                     "beta=0.5, uniform[-1,1)",
@@ -410,6 +415,7 @@ def _grouped_leg(torch, sg, sms, sm_mhz):
         "sequential_ms": round(t_seq, 3), "sequential_gflops": round(flop / t_seq * 1e-6, 1),
         "speedup_vs_sequential": round(t_seq / best, 3),
         "frac_of_simt_peak": round(flop / best * 1e-6 / peak, 4),
+        "roofline_ms": round(roof_ms, 3), "frac_of_roofline": round(roof_ms / best, 4),
         "launches": 1, "tiles": info["tiles"], "work_items_default": info["work_items"],
         "work_items_tuned": tinfo["work_items"], "autotune_s": round(tune_s, 1),
         "tuning": table,
@@ -546,7 +552,7 @@ def run(args):
     if rank == 0 and world == 1 and not args.skip_grouped:
         del A, B, C, C0, flush
         torch.cuda.empty_cache()
-        result["grouped"] = _grouped_leg(torch, sg, sms, sm_max)
+        result["grouped"] = _grouped_leg(torch, sg, sms, sm_max, peaks["hbm_gbs"])
         torch.cuda.empty_cache()
     if rank == 0 and world == 1 and not args.skip_serving:
         result["serving"] = _serving_leg(sg, [500.0, 1000.0, 2000.0, 4000.0], 300)

@@ -269,6 +269,15 @@ int sgemm_b200_fill_random(float* X, int rows, int cols, int ld,
  * expiry (SGEMM_B200_OK or SGEMM_B200_ERR_TIMEOUT).  Synchronises the device. */
 int sgemm_b200_device_status(void);
 
+/* Self-test of the failure path above (no reference counterpart): launches
+ * one thread that waits, bounded by limit_us microseconds (1..10^7), on an
+ * mbarrier phase that nothing completes -- the situation of a TMA copy or MMA
+ * group that never lands -- and records SGEMM_B200_ERR_TIMEOUT in the status
+ * word the way the GEMM kernels do.  The kernel then returns normally; after
+ * `stream` completes, sgemm_b200_device_status() reports the timeout and the
+ * device remains usable.  Returns the launch status. */
+int sgemm_b200_selftest_wait_timeout(int limit_us, sgemm_b200_stream_t stream);
+
 /* Status of the most recent call on this thread (used by sgemm(), which
  * returns void like the reference). */
 int sgemm_b200_last_status(void);

@@ -7,7 +7,10 @@
 // `acc *= alpha; acc += c * beta` evaluated the way nvcc contracts it in the
 // reference (basic.cuh:21-24): C = fma(acc, alpha, c * beta).  Outputs equal
 // the reference kernel's bit for bit.  Like the reference it always reads C.
+//
+// Also here: the bounded-wait self-test (sgemm_b200_selftest_wait_timeout).
 #include "common.h"
+#include "ptx.cuh"
 #include "rng.h"
 
 namespace sgb {
@@ -34,7 +37,40 @@ __global__ void fill_kernel(float* X, int rows, int cols, int ld, uint64_t seed,
     }
 }
 
+// The failure path every TMA/MMA wait in the GEMM kernels takes, run on
+// purpose: one thread waits, bounded by limit_ns of wall time, for an mbarrier
+// phase that nothing will ever complete (no copy and no arrival is issued),
+// then records SGEMM_B200_ERR_TIMEOUT in the status word as the GEMM kernels
+// do, and returns.  Nothing faults and nothing hangs; the context stays usable.
+__global__ void wait_selftest_kernel(int* status, uint64_t limit_ns) {
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x != 0) return;
+    mbar_init(&bar, 1);
+    fence_barrier_init();
+    if (!mbar_wait_for(&bar, 0, limit_ns)) atomicExch(status, SGEMM_B200_ERR_TIMEOUT);
+}
+
 }  // namespace sgb
+
+extern "C" int sgemm_b200_selftest_wait_timeout(int limit_us, sgemm_b200_stream_t stream) {
+    if (limit_us <= 0 || limit_us > 10000000) {
+        sgb::set_last_status(SGEMM_B200_ERR_INVALID_ARG);
+        return SGEMM_B200_ERR_INVALID_ARG;
+    }
+    int s = SGEMM_B200_OK;
+    int* status = sgb::device_status_ptr();
+    if (!sgb::device_is_sm100())
+        s = SGEMM_B200_ERR_UNSUPPORTED;
+    else if (!status)
+        s = SGEMM_B200_ERR_CUDA;
+    else {
+        sgb::wait_selftest_kernel<<<1, 32, 0, sgb::as_stream(stream)>>>(
+            status, static_cast<uint64_t>(limit_us) * 1000ull);
+        s = sgb::cuda_status(cudaGetLastError());
+    }
+    sgb::set_last_status(s);
+    return s;
+}
 
 extern "C" int sgemm_b200_basic(int m, int n, int k, const float* alpha, const float* A, int lda,
                                 const float* B, int ldb, const float* beta, float* C, int ldc,

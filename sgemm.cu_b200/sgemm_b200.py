@@ -121,6 +121,7 @@ def _declare(lib: ctypes.CDLL) -> None:
     d("sgemm_b200_autotune_grouped", _I, [ctypes.POINTER(Problem), _I, ctypes.c_char_p])
     d("sgemm_b200_fill_random", _I, [_P, _I, _I, _I, ctypes.c_uint64, ctypes.c_uint32, _I, _P])
     d("sgemm_b200_device_status", _I, [])
+    d("sgemm_b200_selftest_wait_timeout", _I, [_I, _P])
     d("sgemm_b200_last_status", _I, [])
     d("sgemm_b200_status_string", ctypes.c_char_p, [_I])
     d("sgemm_b200_version", ctypes.c_char_p, [])
@@ -293,6 +294,12 @@ def select_config(m: int, n: int, k: int, A=None, lda: int = 0, B=None, ldb: int
     pa = A.data_ptr() if A is not None else 16
     pb = B.data_ptr() if B is not None else 16
     return lib().sgemm_b200_select_config(m, n, k, pa, lda or k, pb, ldb or n, None, n)
+
+
+def selftest_wait_timeout(limit_us: int, stream=None) -> None:
+    """Run the bounded-wait failure path once (see include/sgemm_b200.h)."""
+    _check(lib().sgemm_b200_selftest_wait_timeout(limit_us, _stream_ptr(stream)),
+           "sgemm_b200_selftest_wait_timeout")
 
 
 def device_status() -> int:

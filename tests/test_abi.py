@@ -114,3 +114,10 @@ def test_host_entry_validation_and_bands():
             assert (r % 128 == 0 and 128 <= r <= m) or r == m
             assert -(-m // r) <= 16
             assert c == n or (c % 128 == 0 and c >= 512 and -(-n // c) <= 4)
+
+
+def test_selftest_wait_validation():
+    # limits outside 1..10^7 microseconds are refused before any device work
+    assert sg.lib().sgemm_b200_selftest_wait_timeout(0, None) == sg.ERR_INVALID_ARG
+    assert sg.lib().sgemm_b200_selftest_wait_timeout(-5, None) == sg.ERR_INVALID_ARG
+    assert sg.lib().sgemm_b200_selftest_wait_timeout(10000001, None) == sg.ERR_INVALID_ARG
