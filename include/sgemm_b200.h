@@ -80,7 +80,7 @@ int sgemm_b200_with_config(int cfg, int m, int n, int k,
                            sgemm_b200_stream_t stream);
 
 /* Number of compiled plain-path kernel configurations and their names
- * (e.g. "tma_128x256_s4"). */
+ * (e.g. "tma_128x64_w4_t8x8_s3"). */
 int sgemm_b200_config_count(void);
 const char* sgemm_b200_config_name(int cfg);
 /* Configuration the dispatcher picks for this shape and these pointers. */
@@ -111,7 +111,8 @@ size_t sgemm_b200_split_workspace_size(int path, int m, int n, int k);
  * (path TF32X3) terms whose cross products run on tcgen05 with FP32
  * accumulation in tensor memory.  Same argument meaning as sgemm_b200.
  * workspace may be NULL, in which case the call allocates it stream-ordered
- * (cudaMallocAsync/cudaFreeAsync on `stream`). */
+ * on `stream` from a memory pool the library keeps per device (freed blocks
+ * are reused by later calls). */
 int sgemm_b200_split(int path, int m, int n, int k,
                      const float* alpha,
                      const float* A, int lda,

@@ -611,7 +611,9 @@ static cudaError_t grow(T** d, T** h, size_t* cap, size_t need, cudaStream_t s) 
         cudaFreeHost(*h);
         *h = nullptr;
     }
-    cudaError_t e = cudaMallocAsync(reinterpret_cast<void**>(d), n * sizeof(T), s);
+    cudaMemPool_t pool = library_pool();
+    if (!pool) return cudaErrorMemoryAllocation;
+    cudaError_t e = cudaMallocFromPoolAsync(reinterpret_cast<void**>(d), n * sizeof(T), pool, s);
     if (e == cudaSuccess && h) e = cudaMallocHost(reinterpret_cast<void**>(h), n * sizeof(T));
     if (e == cudaSuccess) *cap = n;
     return e;
