@@ -18,6 +18,11 @@ by its own CUDA events with an L2-sized flush write in between steps.
                workload; the same leg checks the GPU rows bit for bit
   split        BF16x6 / TF32x3 tensor-core paths on the same 8192^3 problem,
                GFLOP/s and error against FP64 on sampled rows
+  split_configs  plain / BF16x6 / TF32x3 at 8192^3 and 16384^3 with entries
+               sign * 2^e * U[1,2), GFLOP/s and FP64-checked error
+  grouped, serving  the 512-problem grouped launch and the Poisson serving loop
+All FP64 checks run inside the cpu_baseline leg (the oracle is the checker
+there); the other legs only collect sampled output rows.
 
 `--impl reference` runs the reference's own sgemm() (its 128x256x8 kernel at
 this size) built from its sources for sm_100a, same workload and metric.
@@ -250,9 +255,13 @@ def _e2e_host(torch, sg, steps, warmup, size):
     return ms, 3 * size * size * 4, size * size * 4, sg.host_plan(size, size, size)
 
 
-def _cpu_baseline_and_parity(torch, sg, C_after, C0_host, size, target_s=10.0):
-    """Oracle (kernel_basic restatement) on a bounded sample of rows of the same
-    GEMM: its timing is the CPU baseline, its output checks the GPU bit for bit."""
+def _cpu_baseline_and_checks(torch, sg, C_after, C0_host, size, checks, target_s=10.0):
+    """The CPU leg, where the oracle runs as the checker.  The oracle
+    (kernel_basic restatement) on a bounded sample of rows of the same GEMM:
+    its timing is the CPU baseline and its output checks the GPU bit for bit.
+    Then the FP64 error of every sampled GPU output the other legs collected
+    (`checks`: label, size, input distribution, row ids, {path: rows}), from
+    rows regenerated with the oracle's copy of the seeded generator."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
     hA = oracle.fill(size, size, SEED, 1, 0)
@@ -280,6 +289,16 @@ def _cpu_baseline_and_parity(torch, sg, C_after, C0_host, size, target_s=10.0):
     sub = rows[np.linspace(0, nrows - 1, min(256, nrows)).astype(np.int64)]
     ref, mag = oracle.dgemm(hA, hB, C0_host[sub], ALPHA, BETA, row_ids=sub)
     err = oracle.error_stats(C_after[sub], ref, mag)
+    errors = {}
+    for label, n_size, dist, ids, outs in checks:
+        hB_chk = hB if (n_size == size and dist == 0) else oracle.fill(n_size, n_size, SEED, 2,
+                                                                        dist)
+        a_rows = oracle.fill_rows(ids, n_size, SEED, 1, dist)
+        c0_rows = oracle.fill_rows(ids, n_size, SEED, 3, dist)
+        ref_c, mag_c = oracle.dgemm(a_rows, hB_chk, c0_rows, ALPHA, BETA)
+        errors[label] = {path: {k: float(v) for k, v in
+                                oracle.error_stats(rows_out, ref_c, mag_c).items()}
+                         for path, rows_out in outs.items()}
     return {
         "value": round(gflops, 2), "unit": "GFLOP/s", "cores": threads, "kind": "port",
         "sample": f"{nrows} of {size} rows of the {size}^3 GEMM (C restatement of the "
@@ -287,21 +306,15 @@ def _cpu_baseline_and_parity(torch, sg, C_after, C0_host, size, target_s=10.0):
         "seconds": round(dt, 2),
         "parity": {"rows_checked": nrows, "elements": int(got.size), "bit_exact": exact},
         "plain_error_vs_fp64": {"rows": int(len(sub)), **{k: float(v) for k, v in err.items()}},
-    }, (hA, hB)
+    }, errors
 
 
-def _split_leg(torch, sg, A, B, C0, flush, steps, warmup, rows, host_ab, peaks, local):
-    """BF16x6 / TF32x3 on the same problem: GFLOP/s and (when the host copies of
-    A and B exist) FP64 error on sampled rows."""
-    out = {}
+def _split_leg(torch, sg, A, B, C0, flush, steps, warmup, rows, peaks, local):
+    """BF16x6 / TF32x3 on the same problem: GFLOP/s against the tensor-core
+    roofline, plus sampled output rows (C after one call from C0) that the
+    cpu_baseline leg checks against FP64."""
+    out, samples = {}, {}
     idx = torch.from_numpy(rows).long().cuda()
-    ref = mag = None
-    if host_ab is not None:
-        sys.path.insert(0, os.path.join(ROOT, "oracle"))
-        import oracle
-        hA, hB = host_ab
-        C0_rows = C0[idx].cpu().numpy()
-        ref, mag = oracle.dgemm(hA, hB, C0_rows, ALPHA, BETA, row_ids=rows)
     for name in ("bf16x6", "tf32x3"):
         path = sg.PATHS[name]
         try:
@@ -310,10 +323,7 @@ def _split_leg(torch, sg, A, B, C0, flush, steps, warmup, rows, host_ab, peaks, 
             C = C0.clone()
             sg.sgemm_split(path, A, B, C, ALPHA, BETA, workspace=ws)
             torch.cuda.synchronize()
-            err = None
-            if ref is not None:
-                err = {k: float(v) for k, v in
-                       oracle.error_stats(C[idx].cpu().numpy(), ref, mag).items()}
+            samples[name] = C[idx].cpu().numpy()
 
             def run():
                 sg.sgemm_split(path, A, B, C, ALPHA, BETA, workspace=ws)
@@ -339,11 +349,49 @@ def _split_leg(torch, sg, A, B, C0, flush, steps, warmup, rows, host_ab, peaks, 
                                           "the power cap) / products; TF32 taken as half the "
                                           "BF16 rate",
                          "clocks": clk,
-                         "error_vs_fp64_sampled_rows": err}
+                         "error_vs_fp64_sampled_rows": None}
             del ws
         except Exception as e:  # report, never hide
             out[name] = {"error": str(e)}
-    return out
+    return out, samples
+
+
+def _split_configs_leg(torch, sg, sizes, steps, n_rows=32):
+    """The split-precision config: M=N=K in `sizes`, entries sign * 2^e * U[1,2)
+    with e uniform in [-10, 10]; plain, BF16x6 and TF32x3 GFLOP/s, and sampled
+    output rows for the cpu_baseline leg's FP64 check."""
+    out, checks = {}, []
+    for size in sizes:
+        X = [torch.empty((size, size), device="cuda") for _ in range(3)]
+        for tag, M in zip((1, 2, 3), X):
+            sg.fill_random(M, SEED, tag, sg.DIST_SIGNED_POW2)
+        A, B, C0 = X
+        flush = torch.empty((256 << 20) // 4, device="cuda")
+        ids = np.linspace(0, size - 1, n_rows).astype(np.int32)
+        idx = torch.from_numpy(ids).long().cuda()
+        row = {}
+        samples = {}
+        for name in ("plain", "bf16x6", "tf32x3"):
+            C = C0.clone()
+            if name == "plain":
+                run = lambda: sg.sgemm(A, B, C, ALPHA, BETA)  # noqa: E731
+            else:
+                run = lambda p=name: sg.gemm(p, A, B, C, ALPHA, BETA)  # noqa: E731
+            run()
+            torch.cuda.synchronize()
+            samples[name] = C[idx].cpu().numpy()
+            ms = _time_steps(torch, run, steps, 2, flush)
+            t = statistics.mean(ms)
+            row[name] = {"gflops": round(2.0 * size ** 3 / (t * 1e-3) * 1e-9, 1),
+                         "ms_per_step": round(t, 3), "error_vs_fp64_sampled_rows": None}
+            del C
+        for name in ("bf16x6", "tf32x3"):
+            row[name]["speedup_vs_plain"] = round(row[name]["gflops"] / row["plain"]["gflops"], 2)
+        out[str(size)] = row
+        checks.append((f"pow2_{size}", size, sg.DIST_SIGNED_POW2, ids, samples))
+        del A, B, C0, X, flush
+        torch.cuda.empty_cache()
+    return out, checks
 
 
 def _grouped_workload(n, seed):
@@ -540,15 +588,33 @@ def run(args):
                              "value": round(flops * world / (seq_ms * 1e-3) * 1e-9, 1),
                              "ms_per_step": round(seq_ms, 3)}}
 
-    host_ab = None
-    if rank == 0 and world == 1 and not args.skip_cpu:
-        cpu, host_ab = _cpu_baseline_and_parity(torch, sg, C_after, C0_host, SIZE,
-                                                target_s=args.cpu_seconds)
-        result["cpu_baseline"] = cpu
+    checks = []
+    split_rows = np.linspace(0, SIZE - 1, 64).astype(np.int32)
     if rank == 0 and not args.skip_split:
-        result["split"] = _split_leg(torch, sg, A, B, C0, flush, max(20, 2 * args.steps),
-                                     args.warmup, np.linspace(0, SIZE - 1, 64).astype(np.int32),
-                                     host_ab, peaks, local)
+        result["split"], samples = _split_leg(torch, sg, A, B, C0, flush,
+                                              max(20, 2 * args.steps), args.warmup, split_rows,
+                                              peaks, local)
+        if samples:
+            samples["plain"] = C_after[split_rows]
+            checks.append((f"uniform_{SIZE}", SIZE, 0, split_rows, samples))
+        if world == 1 and not args.skip_split_configs:
+            result["split_configs"], more = _split_configs_leg(torch, sg, (8192, 16384), 3)
+            result["split_configs"]["dist"] = "sign * 2^e * U[1,2), e uniform in [-10, 10], seed 0"
+            checks += more
+    if rank == 0 and world == 1 and not args.skip_cpu:
+        cpu, errors = _cpu_baseline_and_checks(torch, sg, C_after, C0_host, SIZE, checks,
+                                               target_s=args.cpu_seconds)
+        result["cpu_baseline"] = cpu
+        uni = errors.get(f"uniform_{SIZE}", {})
+        for name in ("bf16x6", "tf32x3"):
+            if name in uni and isinstance(result.get("split", {}).get(name), dict):
+                result["split"][name]["error_vs_fp64_sampled_rows"] = uni[name]
+        if "plain" in uni and "split" in result:
+            result["split"]["plain_error_vs_fp64_same_rows"] = uni["plain"]
+        for label, errs in errors.items():
+            if label.startswith("pow2_"):
+                for name, e in errs.items():
+                    result["split_configs"][label[5:]][name]["error_vs_fp64_sampled_rows"] = e
     if rank == 0 and world == 1 and not args.skip_grouped:
         del A, B, C, C0, flush
         torch.cuda.empty_cache()
@@ -626,6 +692,8 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-split", action="store_true")
+    ap.add_argument("--skip-split-configs", action="store_true",
+                    help="skip the 8192^3 / 16384^3 signed-power-of-two split configs")
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--skip-grouped", action="store_true")
     ap.add_argument("--skip-serving", action="store_true")
