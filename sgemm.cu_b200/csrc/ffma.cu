@@ -20,6 +20,10 @@ using C3 = Cfg<64, 128, 2, 2, 8, 4, kLoaderTma, 2>;          // 4 warps,  96 KB,
 using C4 = Cfg<64, 64, 2, 1, 8, 4, kLoaderTma, 3>;           // 2 warps,  64 KB, 3/SM
 using C5 = Cfg<64, 128, 2, 2, 8, 3, kLoaderTma, 3>;          // 4 warps,  72 KB, 3/SM
 using C6 = Cfg<128, 64, 4, 1, 8, 3, kLoaderTma, 3>;          // 4 warps,  72 KB, 3/SM
+// Small tiles with 8 x 4 threads, for problems that leave most SMs idle with
+// the tiles above (shared memory limits them to 3 and 4 CTAs/SM).
+using C7 = Cfg<64, 64, 2, 2, 4, 4, kLoaderTma, 4>;         // 4 warps,  64 KB
+using C10 = Cfg<32, 64, 1, 2, 4, 4, kLoaderTma, 6>;        // 2 warps,  48 KB
 using C8 = Cfg<128, 256, 4, 2, 16, 4, kLoaderAsync4, 1>;
 using C9 = Cfg<128, 128, 4, 2, 8, 3, kLoaderAsync4, 2>;
 using C11 = Cfg<64, 128, 2, 2, 8, 4, kLoaderAsync4, 2>;
@@ -41,17 +45,18 @@ constexpr ConfigDesc describe(const char* name, float eff) {
 
 // Efficiencies: relative per-SM throughput of a full wave, normalised to the
 // best configuration of the same loader (TMA: tma_128x64_w4_t8x8_s3;
-// cp.async: cpa_128x256_w8_t8x16_s4).  First measured at 8192^3 / 16384^3
-// (the 8 x 16-thread tiles at 4096^3, where their longer fill and drain costs
-// them most), then checked against a B200 sweep of 256..16384 cubes with the
-// packed-FMA kernels: with plain_select's wave model the pick is within 2.1%
-// of the fastest configuration at every size and 0.2% on average, and a grid
-// refit of these numbers does no better.
+// cp.async: cpa_128x256_w8_t8x16_s4).  The large tiles were measured at
+// 8192^3 / 16384^3 (the 8 x 16-thread tiles at 4096^3, where their longer
+// fill and drain costs them most); the small tiles and the partial-wave
+// fractions in plain_select were then fitted to a B200 sweep of 256..16384
+// cubes: with them the model picks the fastest measured configuration at
+// every size of that sweep.
 static const ConfigDesc kConfigs[] = {
     describe<C0>("tma_128x256_w8_t8x16_s4", 0.840f),   describe<C1>("tma_128x128_w8_t8x8_s3", 0.925f),
     describe<C2>("tma_128x128_w4_t8x16_s3", 0.875f),   describe<C3>("tma_64x128_w4_t8x8_s4", 0.952f),
-    describe<C4>("tma_64x64_w2_t8x8_s4", 0.815f),      describe<C5>("tma_64x128_w4_t8x8_s3", 0.994f),
-    describe<C6>("tma_128x64_w4_t8x8_s3", 1.000f),     describe<C8>("cpa_128x256_w8_t8x16_s4", 1.000f),
+    describe<C4>("tma_64x64_w2_t8x8_s4", 0.700f),      describe<C5>("tma_64x128_w4_t8x8_s3", 0.994f),
+    describe<C6>("tma_128x64_w4_t8x8_s3", 1.000f),     describe<C7>("tma_64x64_w4_t8x4_s4", 0.900f),
+    describe<C10>("tma_32x64_w2_t8x4_s4", 0.700f),     describe<C8>("cpa_128x256_w8_t8x16_s4", 1.000f),
     describe<C9>("cpa_128x128_w8_t8x8_s3", 0.920f),    describe<C11>("cpa_64x128_w4_t8x8_s4", 0.810f),
     describe<C12>("cpa_64x64_w2_t8x8_s4", 0.630f),     describe<C14>("cpa_128x64_w4_t8x8_s3", 0.890f),
 };
@@ -102,11 +107,11 @@ int plain_config_tile(int cfg, int* bm, int* bn) {
 // by occ CTAs).  The last, partial wave leaves r = ceil(remainder / SMs) < occ
 // CTAs on the busiest SM, which then runs at a fraction e(r) of its full
 // throughput (fewer warps to hide latency), so that wave takes
-// t * (r / occ) / e(r).  e(1) = 0.55 and e(2) = 0.85 (of 3) were fitted to
-// B200 sweeps of 768..4096 cubes, where the tile counts leave partial waves.
+// t * (r / occ) / e(r).  e(1) = 0.65, e(2) = 0.85, e(3) = 0.925 were fitted
+// to the same B200 sweep as the efficiencies.
 static double partial_wave_cost(int r, int occ) {
     if (r >= occ) return 1.0;
-    const double e = r == 1 ? 0.55 : 0.85;
+    const double e = r == 1 ? 0.65 : r == 2 ? 0.85 : 0.925;
     return (double(r) / occ) / e;
 }
 
