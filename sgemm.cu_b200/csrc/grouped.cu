@@ -42,25 +42,36 @@ namespace grouped {
 
 using ffma::Operands;
 
-// Two tile shapes of the plain path's 4-warp, 8 x 8 thread-tile FFMA core
-// share one kernel (same thread count, same 24 KB stage, ~168 registers):
-// 3 stages fit 3 CTAs per SM, 4 stages fit 2.
+// Three tile shapes of the plain path's 4-warp FFMA core share one kernel
+// (same thread count, one 24 KB shared-memory slot per stage): 128 x 64 and
+// 64 x 128 with 8 x 8 threads, and 32 x 128 with 8 x 4 threads for problems
+// only a few rows tall, whose rows a 64- or 128-row tile would mostly pad
+// with zeros.  3 stages fit 3 CTAs per SM, 4 stages fit 2.
 template <int S>
 using CfgT = ffma::Cfg<128, 64, 4, 1, 8, S, ffma::kLoaderTma, (S == 3 ? 3 : 2)>;  // 128 x 64
 template <int S>
 using CfgW = ffma::Cfg<64, 128, 2, 2, 8, S, ffma::kLoaderTma, (S == 3 ? 3 : 2)>;  // 64 x 128
+template <int S>
+using CfgS = ffma::Cfg<32, 128, 1, 4, 4, S, ffma::kLoaderTma, (S == 3 ? 3 : 2)>;  // 32 x 128
 
 constexpr int THREADS = 128;
-constexpr int SLOT_BYTES = 24 * 1024;  // both shapes: 16 KB + 8 KB per 32-deep k block
-static_assert(CfgT<3>::STAGE_BYTES == SLOT_BYTES && CfgW<3>::STAGE_BYTES == SLOT_BYTES, "");
-enum TileShape { kTileTall = 0, kTileWide = 1 };  // 128 x 64, 64 x 128
+constexpr int SLOT_BYTES = 24 * 1024;  // 16 KB + 8 KB per 32-deep k block (4 + 16 KB skinny)
+static_assert(CfgT<3>::STAGE_BYTES == SLOT_BYTES && CfgW<3>::STAGE_BYTES == SLOT_BYTES &&
+                  CfgS<3>::STAGE_BYTES <= SLOT_BYTES && CfgS<3>::THREADS == THREADS,
+              "");
+enum TileShape { kTileTall = 0, kTileWide = 1, kTileSkinny = 2 };  // 128x64, 64x128, 32x128
 
-inline int tile_bm(int t) { return t == kTileTall ? 128 : 64; }
+inline int tile_bm(int t) { return t == kTileTall ? 128 : t == kTileWide ? 64 : 32; }
 inline int tile_bn(int t) { return t == kTileTall ? 64 : 128; }
+
+// The 32 x 128 tile's throughput relative to the 8 x 8-thread tiles on work
+// that fills both; a problem takes it when its zero-padded area shrinks by
+// more than this factor.
+constexpr double kSkinnyEfficiency = 0.75;
 
 struct GProblem {
     Operands op;
-    int tile;      // kTileTall or kTileWide
+    int tile;      // a TileShape
     int tma;       // tensor maps valid
     int split;     // k splits
     int kbps;      // k blocks per split
@@ -254,6 +265,10 @@ __global__ void __launch_bounds__(THREADS, (S == 3 ? 3 : 2)) grouped_kernel(cons
             ok = pr.tma ? run_item<CfgT<S>, true, S>(gp, pr, it, it.prob, smem, full_bar, g, &last_s)
                         : run_item<CfgT<S>, false, S>(gp, pr, it, it.prob, smem, full_bar, g,
                                                       &last_s);
+        } else if (pr.tile == kTileSkinny) {
+            ok = pr.tma ? run_item<CfgS<S>, true, S>(gp, pr, it, it.prob, smem, full_bar, g, &last_s)
+                        : run_item<CfgS<S>, false, S>(gp, pr, it, it.prob, smem, full_bar, g,
+                                                      &last_s);
         } else {
             ok = pr.tma ? run_item<CfgW<S>, true, S>(gp, pr, it, it.prob, smem, full_bar, g, &last_s)
                         : run_item<CfgW<S>, false, S>(gp, pr, it, it.prob, smem, full_bar, g,
@@ -437,7 +452,16 @@ static int make_schedule(const sgemm_b200_problem* probs, int count, const Table
         g.op.vec_c = (q.ldc % 4 == 0) && (reinterpret_cast<uintptr_t>(q.C) % 16 == 0);
         const Choice ch = table.c[bucket_of(q.m, q.n, q.k)];
         g.tile = ch.tile;
-        const int bm = tile_bm(ch.tile), bn = tile_bn(ch.tile);
+        {
+            // A problem a few rows tall runs on the 32 x 128 tile when that
+            // removes enough zero padding to pay for the narrower thread tile.
+            auto area = [&](int t) {
+                return double(div_up(q.m, tile_bm(t)) * tile_bm(t)) *
+                       double(div_up(q.n, tile_bn(t)) * tile_bn(t));
+            };
+            if (area(kTileSkinny) < kSkinnyEfficiency * area(ch.tile)) g.tile = kTileSkinny;
+        }
+        const int bm = tile_bm(g.tile), bn = tile_bn(g.tile);
         g.tma = tma_ok(q) ? 1 : 0;
         const int nk = div_up(q.k, 32);
         int split = std::max(1, std::min(ch.split, nk));

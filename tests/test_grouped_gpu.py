@@ -118,6 +118,49 @@ def test_grouped_split_k_deterministic_and_accurate(tmp_path, split):
     plan.close()
 
 
+SKINNY = [(16, 4096, 4096), (1, 1000, 300), (31, 129, 1000), (33, 4100, 64), (48, 640, 2048),
+          (8, 8, 8), (20, 3000, 3001), (200, 300, 50)]
+
+
+def test_grouped_skinny_tiles_bit_exact_with_plain_path():
+    # tall-skinny problems (the serving loop's common case) run on 32 x 128
+    # tiles; every element keeps the plain path's FMA chain, so bits agree
+    torch = _torch()
+    lds = [(None, None, None)] * (len(SKINNY) - 1) + [(53, 307, 301)]
+    specs, host = _make(SKINNY, 700, lds)
+    plan = sg.GroupedPlan(specs)
+    plan.launch(use_graph=True)
+    torch.cuda.synchronize()
+    assert sg.device_status() == sg.OK
+    for (dA, dB, dC, a, b), (A, B, C, _, _) in zip(specs, host):
+        want = oracle.sgemm_basic(A, B, C, a, b, basic=False)
+        assert np.array_equal(dC.cpu().numpy(), want), f"{A.shape}x{B.shape}"
+    plan.close()
+
+
+def test_grouped_skinny_split_k_deterministic_and_accurate(tmp_path):
+    torch = _torch()
+    shapes = [(16, 1024, 4096), (40, 520, 3000)]
+    specs, host = _make(shapes, 800)
+    C0 = [s[2].clone() for s in specs]
+    plan = sg.GroupedPlan(specs, tuning_json=_table(tmp_path / "t.json", 4))
+    assert plan.info()["work_items"] > plan.info()["tiles"]
+    plan.launch()
+    torch.cuda.synchronize()
+    first = [s[2].clone() for s in specs]
+    for s, c in zip(specs, C0):
+        s[2].copy_(c)
+    plan.launch()
+    torch.cuda.synchronize()
+    for s, f, (A, B, C, a, b) in zip(specs, first, host):
+        assert torch.equal(s[2], f)
+        ref, mag = oracle.dgemm(A, B, C, a, b)
+        e = oracle.error_stats(f.cpu().numpy(), ref, mag)
+        ep = oracle.error_stats(oracle.sgemm_basic(A, B, C, a, b, basic=False), ref, mag)
+        assert e["max_componentwise"] <= 1.5 * ep["max_componentwise"] + 2.0 ** -23
+    plan.close()
+
+
 def _workload(n, seed):
     """M, N, K log-uniform on [64, 4096], multiples of 8."""
     rng = np.random.default_rng(seed)

@@ -41,3 +41,14 @@ def test_schedule_rejects_bad_problem():
     with pytest.raises(sg.SgemmError) as e:
         sg.grouped_schedule(probs)
     assert e.value.status == sg.ERR_INVALID_ARG
+
+
+def test_schedule_uses_skinny_tile_for_short_problems():
+    # problems a few rows tall run on 32 x 128 tiles instead of padding 128-row tiles
+    shapes = [(16, 4096, 4096), (1, 1000, 300), (33, 4100, 64), (48, 640, 2048)]
+    s = sg.grouped_schedule(sg.host_problems(shapes))
+    want = sum(math.ceil(m / 32) * math.ceil(n / 128) for m, n, k in shapes)
+    assert s["tiles"] == want
+    # square problems keep the 8 x 8-thread tiles
+    s = sg.grouped_schedule(sg.host_problems([(256, 256, 256)]))
+    assert s["tiles"] == math.ceil(256 / 128) * math.ceil(256 / 64)
