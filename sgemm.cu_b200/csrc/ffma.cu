@@ -11,7 +11,7 @@
 namespace sgb {
 namespace ffma {
 
-// Compiled configurations.  Index = public config id.
+// Compiled configurations (the public config id is the position in kConfigs).
 //   tile      warps  thread tile  stages  loader   resident CTAs/SM
 using C0 = Cfg<128, 256, 4, 2, 16, 4, kLoaderTma, 1>;        // 8 warps, 192 KB smem, 1/SM
 using C1 = Cfg<128, 128, 4, 2, 8, 3, kLoaderTma, 2>;         // 8 warps,  96 KB, 2/SM
@@ -22,8 +22,8 @@ using C5 = Cfg<64, 128, 2, 2, 8, 3, kLoaderTma, 3>;          // 4 warps,  72 KB,
 using C6 = Cfg<128, 64, 4, 1, 8, 3, kLoaderTma, 3>;          // 4 warps,  72 KB, 3/SM
 // Small tiles with 8 x 4 threads, for problems that leave most SMs idle with
 // the tiles above (shared memory limits them to 3 and 4 CTAs/SM).
-using C7 = Cfg<64, 64, 2, 2, 4, 4, kLoaderTma, 4>;         // 4 warps,  64 KB
-using C10 = Cfg<32, 64, 1, 2, 4, 4, kLoaderTma, 6>;        // 2 warps,  48 KB
+using S0 = Cfg<64, 64, 2, 2, 4, 4, kLoaderTma, 4>;         // 4 warps,  64 KB
+using S1 = Cfg<32, 64, 1, 2, 4, 4, kLoaderTma, 6>;         // 2 warps,  48 KB
 using C8 = Cfg<128, 256, 4, 2, 16, 4, kLoaderAsync4, 1>;
 using C9 = Cfg<128, 128, 4, 2, 8, 3, kLoaderAsync4, 2>;
 using C11 = Cfg<64, 128, 2, 2, 8, 4, kLoaderAsync4, 2>;
@@ -55,8 +55,8 @@ static const ConfigDesc kConfigs[] = {
     describe<C0>("tma_128x256_w8_t8x16_s4", 0.840f),   describe<C1>("tma_128x128_w8_t8x8_s3", 0.925f),
     describe<C2>("tma_128x128_w4_t8x16_s3", 0.875f),   describe<C3>("tma_64x128_w4_t8x8_s4", 0.952f),
     describe<C4>("tma_64x64_w2_t8x8_s4", 0.700f),      describe<C5>("tma_64x128_w4_t8x8_s3", 0.994f),
-    describe<C6>("tma_128x64_w4_t8x8_s3", 1.000f),     describe<C7>("tma_64x64_w4_t8x4_s4", 0.900f),
-    describe<C10>("tma_32x64_w2_t8x4_s4", 0.700f),     describe<C8>("cpa_128x256_w8_t8x16_s4", 1.000f),
+    describe<C6>("tma_128x64_w4_t8x8_s3", 1.000f),     describe<S0>("tma_64x64_w4_t8x4_s4", 0.900f),
+    describe<S1>("tma_32x64_w2_t8x4_s4", 0.700f),      describe<C8>("cpa_128x256_w8_t8x16_s4", 1.000f),
     describe<C9>("cpa_128x128_w8_t8x8_s3", 0.920f),    describe<C11>("cpa_64x128_w4_t8x8_s4", 0.810f),
     describe<C12>("cpa_64x64_w2_t8x8_s4", 0.630f),     describe<C14>("cpa_128x64_w4_t8x8_s3", 0.890f),
 };
