@@ -401,10 +401,10 @@ def _grouped_workload(n, seed):
     return [tuple(int(max(8, round(v / 8) * 8)) for v in row) for row in vals]
 
 
-def _grouped_leg(torch, sg, sms, sm_mhz, hbm_gbs):
-    """One persistent graph-captured launch over 512 uneven problems vs 512
-    sequential plain launches; then the autotuned plan."""
-    shapes = _grouped_workload(512, 7)
+def _grouped_leg(torch, sg, sms, sm_mhz, hbm_gbs, count=512):
+    """One persistent graph-captured launch over `count` (512) uneven problems
+    vs as many sequential plain launches; then the autotuned plan."""
+    shapes = _grouped_workload(count, 7)
     specs = []
     for i, (m, n, k) in enumerate(shapes):
         A = torch.empty((m, k), device="cuda")
@@ -454,8 +454,8 @@ def _grouped_leg(torch, sg, sms, sm_mhz, hbm_gbs):
                       4.0 * (m * k + k * n + 2 * m * n) / (hbm_gbs * 1e9))
                   for m, n, k in shapes) * 1e3
     return {
-        "workload": "512 problems, M,N,K log-uniform [64,4096] multiples of 8, alpha=1.5 "
-                    "beta=0.5, uniform[-1,1)",
+        "workload": f"{count} problems, M,N,K log-uniform [64,4096] multiples of 8, "
+                    "alpha=1.5 beta=0.5, uniform[-1,1)",
         "tflop": round(flop * 1e-12, 4),
         "grouped_ms": round(t_grouped, 3), "grouped_gflops": round(flop / t_grouped * 1e-6, 1),
         "grouped_tuned_ms": round(t_tuned, 3),
@@ -618,7 +618,8 @@ def run(args):
     if rank == 0 and world == 1 and not args.skip_grouped:
         del A, B, C, C0, flush
         torch.cuda.empty_cache()
-        result["grouped"] = _grouped_leg(torch, sg, sms, sm_max, peaks["hbm_gbs"])
+        result["grouped"] = _grouped_leg(torch, sg, sms, sm_max, peaks["hbm_gbs"],
+                                         args.grouped_problems)
         torch.cuda.empty_cache()
     if rank == 0 and world == 1 and not args.skip_serving:
         result["serving"] = _serving_leg(sg, [500.0, 1000.0, 2000.0, 4000.0], 300)
@@ -697,6 +698,9 @@ def main():
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--skip-grouped", action="store_true")
     ap.add_argument("--skip-serving", action="store_true")
+    ap.add_argument("--grouped-problems", type=int, default=512,
+                    help="problems in the grouped leg (default 512; fewer only for profiler "
+                         "captures)")
     ap.add_argument("--size", type=int, default=SIZE,
                     help="M=N=K (default 8192; smaller sizes only for profiler captures)")
     args = ap.parse_args()

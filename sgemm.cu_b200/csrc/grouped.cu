@@ -296,7 +296,7 @@ inline int bucket_of(int m, int n, int k) {
 }
 
 struct Table {
-    int stages = 4;
+    int stages = 3;  // 3 CTAs per SM; the autotuner may pick 4 (2 per SM)
     Choice c[kBuckets];
     Table() {
         for (int a = 0; a < kMnClasses; ++a)
@@ -840,7 +840,8 @@ extern "C" int sgemm_b200_autotune_grouped(const sgemm_b200_problem* problems, i
     double best_ms = measure(best);
     // Stage count (one per launch), then tile shape and split-K per bucket by
     // coordinate descent over the buckets present in the workload.
-    for (int st : {3}) {
+    for (int st : {3, 4}) {
+        if (st == best.stages) continue;
         Table t = best;
         t.stages = st;
         const double ms = measure(t);
