@@ -575,7 +575,7 @@ def run(args):
     # e2e through the C ABI from pinned host buffers (sgemm_b200_host), and the
     # copy -> sgemm() -> copy sequence the reference's callers use, for context
     if not args.skip_e2e:
-        ms_e2e, h2d, d2h, (rows, cols) = _e2e_host(torch, sg, max(3, args.steps // 5), 2, SIZE)
+        ms_e2e, h2d, d2h, (rows, chunks) = _e2e_host(torch, sg, max(3, args.steps // 5), 2, SIZE)
         e2e_ms = _max_over_ranks(dist, ms_e2e)
         ms_seq, _, _ = _e2e(torch, lambda a, b, c: sg.sgemm(a, b, c, ALPHA, BETA),
                             max(3, args.steps // 5), 2, SIZE)
@@ -583,7 +583,8 @@ def run(args):
         result["e2e"] = {"value": round(flops * world / (e2e_ms * 1e-3) * 1e-9, 1),
                          "unit": "GFLOP/s", "ms_per_step": round(e2e_ms, 3),
                          "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                         "api": f"sgemm_b200_host, blocks of {rows} rows x {cols} columns",
+                         "api": f"sgemm_b200_host, bands of {rows} rows x column chunks "
+                                f"{chunks}",
                          "copy_then_sgemm": {
                              "value": round(flops * world / (seq_ms * 1e-3) * 1e-9, 1),
                              "ms_per_step": round(seq_ms, 3)}}

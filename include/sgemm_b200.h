@@ -188,9 +188,12 @@ int sgemm_b200_host(int path, int m, int n, int k,
                     float* C, int ldc,
                     sgemm_b200_stream_t stream);
 
-/* Block shape sgemm_b200_host uses for this problem: rows per band and
- * columns per chunk (m and n when it does not split).  Host-only. */
-int sgemm_b200_host_plan(int path, int m, int n, int k, int reads_c, int* rows, int* cols);
+/* Block plan sgemm_b200_host uses for this problem (host-only): writes the
+ * rows per band to *rows and the widths of up to max_chunks column chunks to
+ * chunk_cols, and returns the number of chunks (m rows and one chunk of n
+ * columns when it does not split), or a negated sgemm_b200_status. */
+int sgemm_b200_host_plan(int path, int m, int n, int k, int reads_c, int* rows,
+                         int* chunk_cols, int max_chunks);
 
 /* ------------------------------------------------------------------------ */
 /* Grouped persistent GEMM (no reference counterpart)                        */

@@ -5,8 +5,8 @@
 // benchmark.cu:69-73), so the PCIe transfers and the kernel run one after the
 // other.  Here the library stages the operands through HBM itself and overlaps
 // the three phases.  C is cut into blocks: row bands (at most 16, multiples of
-// 128 rows) times column chunks (1..4, multiples of 128 columns); the blocks
-// go column chunk by column chunk:
+// 128 rows) times column chunks (1..4, of planned widths); the blocks go
+// column chunk by column chunk:
 //
 //   copy stream (H2D):  B[:, chunk j], then per row band b: A[b, :] (first
 //                       chunk only) and, when beta != 0, C[b, chunk j]
@@ -15,10 +15,10 @@
 //                       overlaps its neighbours' copies and wave tails
 //   copy stream (D2H):  C[b, chunk j] back to the host once computed
 //
-// Column chunks let the first kernel start after 1/S of B instead of all of
-// it; the number of chunks comes from a small timing model of this pipeline
+// Column chunks let the first kernel start after part of B instead of all
+// of it; the chunk widths come from a small timing model of this pipeline
 // (PCIe bandwidth and per-path GEMM rate measured on a B200), evaluated for
-// 1..4 chunks per call.  Every block is the same GEMM on a sub-matrix, issued
+// even and uneven splits per call.  Every block is the same GEMM on a sub-matrix, issued
 // through sgemm_b200_gemm(); each C element keeps its k-ordered accumulation,
 // so the result is bit-identical to copying the whole matrices and calling the
 // device entry point once.
@@ -99,29 +99,30 @@ static int band_rows(int m, int cols) {
     return std::min(m, r);
 }
 
-// Columns per chunk for `chunks` chunks: a multiple of 128, the last chunk
-// takes the rest.
-static int chunk_cols(int n, int chunks) {
-    if (chunks <= 1) return n;
-    const int c = (n + chunks - 1) / chunks;
-    return std::min(n, (c + 127) / 128 * 128);
-}
+// A plan: row bands of `rows` rows (the last takes the rest) times up to
+// kMaxChunks column chunks of the given widths (multiples of 128 but the
+// last), taken chunk by chunk.
+struct Plan {
+    int rows;
+    int nchunks;
+    int cols[kMaxChunks];
+};
 
 // Timing model of the pipeline: one H2D queue, one D2H queue, and the GEMMs
 // as one server at the path's rate.  Constants measured on a B200 (pinned
 // host memory; GEMM rates at 8192^3).
-static double model_ms(int path, int m, int n, int k, bool read_c, int rows, int cols) {
+static double model_ms(int path, int m, int k, bool read_c, const Plan& p) {
     constexpr double kPcieBytesPerS = 51e9;
     const double flops_per_s = path == SGEMM_B200_PATH_BF16X6   ? 225e12
                                : path == SGEMM_B200_PATH_TF32X3 ? 210e12
                                                                 : 59e12;
     double t_h = 0, t_c = 0, t_d = 0;
-    for (int c0 = 0; c0 < n; c0 += cols) {
-        const double nc = std::min(cols, n - c0);
+    for (int j = 0; j < p.nchunks; ++j) {
+        const double nc = p.cols[j];
         t_h += 4.0 * k * nc / kPcieBytesPerS;
-        for (int r0 = 0; r0 < m; r0 += rows) {
-            const double nr = std::min(rows, m - r0);
-            if (c0 == 0) t_h += 4.0 * nr * k / kPcieBytesPerS;
+        for (int r0 = 0; r0 < m; r0 += p.rows) {
+            const double nr = std::min(p.rows, m - r0);
+            if (j == 0) t_h += 4.0 * nr * k / kPcieBytesPerS;
             if (read_c) t_h += 4.0 * nr * nc / kPcieBytesPerS;
             t_c = std::max(t_c, t_h) + 2.0 * nr * nc * k / flops_per_s;
             t_d = std::max(t_d, t_c) + 4.0 * nr * nc / kPcieBytesPerS;
@@ -130,26 +131,49 @@ static double model_ms(int path, int m, int n, int k, bool read_c, int rows, int
     return t_d * 1e3;
 }
 
-struct Plan {
-    int rows, cols;
-};
-
+// Candidates: one chunk; 2..4 even chunks; and two or three uneven chunks
+// with widths in steps of ~n/16.  An uneven plan with a wide first chunk
+// gives each A band that arrives with the first chunk more work, so the
+// phase in which A streams in stays compute-bound; narrow later chunks then
+// start early.  Every chunk is at least 512 columns, and the rows per band
+// keep every block at least kMinBlockElems.
 Plan make_plan(int path, int m, int n, int k, bool read_c) {
     const double bytes = 4.0 * (double(m) * k + double(k) * n + double(m) * n * (read_c ? 2 : 1));
-    if (bytes < 16.0 * (1 << 20)) return Plan{m, n};  // small: one block
-    Plan p{band_rows(m, n), n};
-    double best = model_ms(path, m, n, k, read_c, p.rows, n);
-    for (int s = 2; s <= kMaxChunks; ++s) {
-        const int cols = chunk_cols(n, s);
-        if (cols < 512 || cols >= n) break;
-        const int rows = band_rows(m, cols);
-        const double t = model_ms(path, m, n, k, read_c, rows, cols);
-        if (t < best * 0.98) {  // fewer, larger blocks unless clearly slower
-            best = t;
-            p = Plan{rows, cols};
+    Plan best{m, 1, {n}};
+    if (bytes < 16.0 * (1 << 20)) return best;  // small: one block
+    best.rows = band_rows(m, n);
+    double best_t = model_ms(path, m, k, read_c, best);
+    auto consider = [&](std::initializer_list<int> widths) {
+        Plan p{0, 0, {}};
+        int narrowest = n, used = 0;
+        for (int w : widths) {
+            if (w < 512) return;
+            p.cols[p.nchunks++] = w;
+            used += w;
+            narrowest = std::min(narrowest, w);
         }
+        if (n - used < 512) return;
+        p.cols[p.nchunks++] = n - used;
+        narrowest = std::min(narrowest, n - used);
+        p.rows = band_rows(m, narrowest);
+        const double t = model_ms(path, m, k, read_c, p);
+        if (t < best_t * 0.98) {  // fewer, larger blocks unless clearly faster
+            best_t = t;
+            best = p;
+        }
+    };
+    for (int s = 2; s <= 4; ++s) {  // even chunks
+        const int c = (n + s - 1) / s / 128 * 128;
+        if (s == 2) consider({c});
+        if (s == 3) consider({c, c});
+        if (s == 4) consider({c, c, c});
     }
-    return p;
+    const int g = std::max(128, (n / 16 + 127) / 128 * 128);
+    for (int a = g; a < n; a += g) {  // uneven: first chunk a, then b, then the rest
+        consider({a});
+        for (int b2 = g; a + b2 < n; b2 += g) consider({a, b2});
+    }
+    return best;
 }
 
 static int run(int path, int m, int n, int k, const float* alpha, const float* A, int lda,
@@ -163,7 +187,6 @@ static int run(int path, int m, int n, int k, const float* alpha, const float* A
     const bool read_c = *beta != 0.0f;  // beta == 0: C is written, never read
     const Plan plan = make_plan(path, m, n, k, read_c);
     const int bands = (m + plan.rows - 1) / plan.rows;
-    const int chunks = (n + plan.cols - 1) / plan.cols;
     // Device pitches: rows start on 16 bytes, so the TMA kernels take every block.
     const int lda_d = (k + 3) / 4 * 4, ldb_d = (n + 3) / 4 * 4, ldc_d = (n + 3) / 4 * 4;
     const size_t a_bytes = align_up(sizeof(float) * (size_t)m * lda_d, 256);
@@ -193,8 +216,8 @@ static int run(int path, int m, int n, int k, const float* alpha, const float* A
         for (cudaStream_t s : all) ok(cudaStreamWaitEvent(s, eng->start, 0));
 
     int blk = 0;
-    for (int j = 0; j < chunks && status == SGEMM_B200_OK; ++j) {
-        const int c0 = j * plan.cols, nc = std::min(plan.cols, n - c0);
+    for (int j = 0, c0 = 0; j < plan.nchunks && status == SGEMM_B200_OK; c0 += plan.cols[j++]) {
+        const int nc = plan.cols[j];
         if (k > 0 && ok(cudaMemcpy2DAsync(dB + c0, f * ldb_d, B + c0, f * ldb, f * nc, k,
                                           cudaMemcpyDefault, eng->h2d)))
             ok(cudaEventRecord(eng->b_in[j], eng->h2d));
@@ -262,10 +285,11 @@ extern "C" int sgemm_b200_host(int path, int m, int n, int k, const float* alpha
 }
 
 extern "C" int sgemm_b200_host_plan(int path, int m, int n, int k, int reads_c, int* rows,
-                                    int* cols) {
-    if (m <= 0 || n <= 0 || k < 0 || !rows || !cols) return SGEMM_B200_ERR_INVALID_ARG;
+                                    int* chunk_cols, int max_chunks) {
+    if (m <= 0 || n <= 0 || k < 0 || !rows || !chunk_cols || max_chunks < 1)
+        return -SGEMM_B200_ERR_INVALID_ARG;
     const sgb::host::Plan p = sgb::host::make_plan(path, m, n, k, reads_c != 0);
     *rows = p.rows;
-    *cols = p.cols;
-    return SGEMM_B200_OK;
+    for (int j = 0; j < p.nchunks && j < max_chunks; ++j) chunk_cols[j] = p.cols[j];
+    return p.nchunks;
 }

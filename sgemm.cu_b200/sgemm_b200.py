@@ -105,7 +105,8 @@ def _declare(lib: ctypes.CDLL) -> None:
     d("sgemm_b200_split", _I, [_I] + _GEMM_ARGS + [_P, ctypes.c_size_t, _P])
     d("sgemm_b200_gemm", _I, [_I] + _GEMM_ARGS + [_P])
     d("sgemm_b200_host", _I, [_I] + _GEMM_ARGS + [_P])
-    d("sgemm_b200_host_plan", _I, [_I, _I, _I, _I, _I, ctypes.POINTER(_I), ctypes.POINTER(_I)])
+    d("sgemm_b200_host_plan", _I, [_I, _I, _I, _I, _I, ctypes.POINTER(_I), ctypes.POINTER(_I),
+                                   _I])
     d("sgemm_b200_grouped_plan_create", _I,
       [ctypes.POINTER(_P), ctypes.POINTER(Problem), _I, ctypes.c_char_p])
     d("sgemm_b200_grouped_plan_launch", _I, [_P, _P, _I])
@@ -270,12 +271,14 @@ def sgemm_host(A, B, C, alpha: float = 1.0, beta: float = 0.0, path="plain",
 
 
 def host_plan(m: int, n: int, k: int, reads_c: bool = True, path="plain") -> tuple:
-    """(rows per band, columns per chunk) sgemm_host uses for this problem."""
+    """(rows per band, [column chunk widths]) sgemm_host uses for this problem."""
     p = PATHS[path] if isinstance(path, str) else int(path)
-    r, c = ctypes.c_int(0), ctypes.c_int(0)
-    _check(lib().sgemm_b200_host_plan(p, m, n, k, int(reads_c), ctypes.byref(r), ctypes.byref(c)),
-           "sgemm_b200_host_plan")
-    return r.value, c.value
+    r = ctypes.c_int(0)
+    cols = (ctypes.c_int * 16)()
+    cnt = lib().sgemm_b200_host_plan(p, m, n, k, int(reads_c), ctypes.byref(r), cols, 16)
+    if cnt < 0:
+        raise SgemmError(-cnt, "sgemm_b200_host_plan")
+    return r.value, [cols[i] for i in range(cnt)]
 
 
 def fill_random(X, seed: int, tag: int, dist: int = DIST_UNIFORM_PM1, stream=None) -> None:

@@ -103,18 +103,19 @@ def test_host_entry_validation_and_bands():
     assert l.sgemm_b200_host(0, 0, 4, 4, ctypes.byref(a), None, 4, None, 4, ctypes.byref(b),
                              None, 4, None) == sg.OK
     # blocking: <= 16 row bands of a multiple of 128 rows, <= 4 column chunks
-    # of a multiple of 128 columns; small problems in one block
-    assert sg.host_plan(8192, 8192, 8192) == (512, 4096)  # the model's pick
-    assert sg.host_plan(4096, 4096, 4096) == (384, 4096)
+    # (widths multiples of 128 but the last, each >= 512 columns); small
+    # problems in one block; the split is the timing model's pick
+    rows, chunks = sg.host_plan(8192, 8192, 8192)
+    assert sum(chunks) == 8192 and len(chunks) >= 2 and rows % 128 == 0
     assert sg.host_plan(200, 8192, 8192)[0] == 200  # one band; B may still be chunked
-    assert sg.host_plan(1000, 1000, 1000) == (1000, 1000)  # < 16 MB moved
+    assert sg.host_plan(1000, 1000, 1000) == (1000, [1000])  # < 16 MB moved
     for m, n in ((3001, 4096), (5003, 5003), (8191, 777), (100000, 4096), (16384, 16384)):
         for path in ("plain", "bf16x6", "tf32x3"):
-            r, c = sg.host_plan(m, n, 4096, True, path)
+            r, chunks = sg.host_plan(m, n, 4096, True, path)
             assert (r % 128 == 0 and 128 <= r <= m) or r == m
-            assert -(-m // r) <= 16
-            assert c == n or (c % 128 == 0 and c >= 512 and -(-n // c) <= 4)
-
+            assert -(-m // r) <= 16 and 1 <= len(chunks) <= 4 and sum(chunks) == n
+            assert all(c % 128 == 0 and c >= 512 for c in chunks[:-1])
+            assert len(chunks) == 1 or chunks[-1] >= 512
 
 def test_selftest_wait_validation():
     # limits outside 1..10^7 microseconds are refused before any device work
