@@ -59,7 +59,10 @@ typedef enum {
  * status return.  Each C element is accumulated over k in increasing order
  * with one fused multiply-add per term, then acc *= alpha and
  * C = fmaf(C_old, beta, acc), so results equal the reference kernels' bit for
- * bit on the same inputs. */
+ * bit on the same inputs.  After one call on the device outside stream
+ * capture (which caches the device's properties and the library pool), calls
+ * can be captured into a CUDA graph, including ones whose unaligned strides
+ * take the pack-to-aligned-rows path (its scratch is stream-ordered). */
 int sgemm_b200(int m, int n, int k,
                const float* alpha,
                const float* A, int lda,

@@ -246,3 +246,34 @@ def test_cpp_harness_sweep(tmp_path):
                         f"--savedir={tmp_path}"], capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
     assert "FAILED: 0" in r.stdout
+
+
+@pytest.mark.parametrize("m,n,k,ld_pad", [(2048, 1536, 1024, 0), (1001, 3001, 777, 1)])
+def test_plain_path_captures_into_a_cuda_graph(m, n, k, ld_pad):
+    # one launch with by-value tensor maps (aligned case) or the pack path's
+    # stream-ordered scratch plus the launch (unaligned case): both capture,
+    # and every replay gives the direct call's bits
+    torch = _torch()
+    A, B, C = _inputs(m, n, k, 17, 0)
+    lds = (k + ld_pad, n + ld_pad, n + ld_pad) if ld_pad else (None, None, None)
+    want = _run_ours(A, B, C, 1.5, 0.5, lds=lds)
+    _, dA = _dev(A, lds[0])
+    _, dB = _dev(B, lds[1])
+    bigC, dC = _dev(C, lds[2])
+    C0 = dC.clone()
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.stream(s):
+        sg.sgemm(dA, dB, dC, 1.5, 0.5, stream=s)  # first call outside capture: lazy set-up
+        s.synchronize()
+        dC.copy_(C0)
+        s.synchronize()
+        with torch.cuda.graph(g, stream=s):
+            sg.sgemm(dA, dB, dC, 1.5, 0.5, stream=s)
+    for _ in range(2):
+        dC.copy_(C0)
+        g.replay()
+        torch.cuda.synchronize()
+        assert np.array_equal(dC.cpu().numpy(), want)
+    del g
