@@ -277,3 +277,35 @@ def test_plain_path_captures_into_a_cuda_graph(m, n, k, ld_pad):
         torch.cuda.synchronize()
         assert np.array_equal(dC.cpu().numpy(), want)
     del g
+
+
+def _special(shape, seed):
+    """U[-1,1) entries with subnormals, exact zeros, signed zeros, magnitudes
+    whose products overflow to +-Inf, and a few NaNs mixed in."""
+    rng = np.random.default_rng(seed)
+    x = rng.uniform(-1, 1, size=shape).astype(np.float32)
+    pick = rng.random(shape)
+    x[pick < 0.05] = (rng.uniform(-1, 1, size=shape) * 1e-39).astype(np.float32)[pick < 0.05]
+    x[(pick >= 0.05) & (pick < 0.08)] = 0.0
+    x[(pick >= 0.08) & (pick < 0.09)] = -0.0
+    x[(pick >= 0.09) & (pick < 0.092)] = np.float32(3e38)
+    x[(pick >= 0.092) & (pick < 0.0925)] = np.nan
+    return x
+
+
+@pytest.mark.parametrize("config", ["default", "cpa"])
+def test_special_values_bit_exact(config):
+    # subnormals are kept (no flush to zero), Inf and NaN propagate: the packed
+    # FMA core rounds exactly like the reference's fmaf chain
+    A = _special((300, 257), 1)
+    B = _special((257, 200), 2)
+    C = _special((300, 200), 3)
+    cfg = -1 if config == "default" else sg.config_names().index("cpa_64x128_w4_t8x8_s4")
+    got = _run_ours(A, B, C, 1.5, 0.5, config=cfg)
+    want = oracle.sgemm_basic(A, B, C, 1.5, 0.5, basic=False)
+    _assert_equal(got, want)
+    # the products of subnormals with ordinary values are subnormal, not zero
+    tiny = np.full((64, 64), 1e-39, np.float32)
+    one = np.eye(64, dtype=np.float32)
+    got = _run_ours(tiny, one, np.zeros((64, 64), np.float32), 1.0, 0.0, config=cfg)
+    assert np.array_equal(got, tiny)
