@@ -309,3 +309,26 @@ def test_special_values_bit_exact(config):
     one = np.eye(64, dtype=np.float32)
     got = _run_ours(tiny, one, np.zeros((64, 64), np.float32), 1.0, 0.0, config=cfg)
     assert np.array_equal(got, tiny)
+
+
+@pytest.mark.parametrize("m,n,k,pad", [(300, 200, 150, 0), (257, 129, 1000, 3), (64, 1000, 33, 8)])
+def test_column_major_callers_swap_operands(m, n, k, pad):
+    # the reference's convention for column-major data (src/sgemm.cuh:31-33):
+    # swap (A, lda) with (B, ldb) and m with n, since C^T = B^T * A^T.  A
+    # column-major m x k array with leading dimension lda is, byte for byte,
+    # a row-major k x m array with row stride lda, so nothing is copied.
+    import ctypes
+
+    torch = _torch()
+    A, B, C = _inputs(m, n, k, 23, 0)
+    want = oracle.sgemm_basic(A, B, C, 1.5, 0.5, basic=False)
+    lda, ldb, ldc = m + pad, k + pad, m + pad
+    _, dAc = _dev(np.ascontiguousarray(A.T), lda)  # A column-major: k rows of lda
+    _, dBc = _dev(np.ascontiguousarray(B.T), ldb)  # B column-major: n rows of ldb
+    bigC, dCc = _dev(np.ascontiguousarray(C.T), ldc)  # C column-major: n rows of ldc
+    a, b = ctypes.c_float(1.5), ctypes.c_float(0.5)
+    st = sg.lib().sgemm_b200(n, m, k, ctypes.byref(a), dBc.data_ptr(), ldb, dAc.data_ptr(), lda,
+                             ctypes.byref(b), dCc.data_ptr(), ldc, None)
+    assert st == sg.OK
+    torch.cuda.synchronize()
+    _assert_equal(np.ascontiguousarray(dCc.cpu().numpy().T), want)
