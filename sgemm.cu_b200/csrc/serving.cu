@@ -325,13 +325,21 @@ static void worker_loop(Server* s) {
             s->max_batch_seen = std::max(s->max_batch_seen, (int)sl.batch.size());
             lock.unlock();
             const int st = launch_batch(s, free_slot);
+            // A launch that failed part-way may have left work on the slot's
+            // stream that still reads or writes the batch's memory: let it
+            // finish before that memory can go to another request.
+            if (st != SGEMM_B200_OK) cudaStreamSynchronize(sl.stream);
             lock.lock();
             if (st != SGEMM_B200_OK) {
-                // The batch never reached the GPU: fail its requests.
+                // Fail the batch's requests.
                 for (Request* r : sl.batch) {
                     r->state = kFailed;
                     ++s->failed;
                     --s->outstanding;
+                    if (r->ready) {
+                        cudaEventDestroy(r->ready);
+                        r->ready = nullptr;
+                    }
                     if (r->auto_release) {
                         pool_free(&s->pool, r->off);
                         r->off = -1;
@@ -433,8 +441,8 @@ extern "C" int sgemm_b200_server_submit(sgemm_b200_server* srv, int m, int n, in
     r->seed = seed;
     r->bytes = sgb::serving::request_bytes(s->cfg.path, m, n, k, &r->ws_bytes);
     r->t_submit = sgb::serving::secs(sgb::serving::Clock::now());
-    r->auto_release = s->cfg.keep_results == 0;
     std::lock_guard<std::mutex> lock(s->mu);
+    r->auto_release = s->cfg.keep_results == 0;
     r->id = s->next_id++;
     s->all[r->id] = r;
     if (id) *id = r->id;
@@ -565,8 +573,13 @@ extern "C" int sgemm_b200_server_run_poisson(sgemm_b200_server* srv, double rate
         s->max_in_flight = s->max_batch_seen = 0;
         s->peak_waiting = 0;
     }
-    const int keep = s->cfg.keep_results;
-    s->cfg.keep_results = 0;  // an open-loop run releases results as they complete
+    int keep;
+    {
+        // an open-loop run releases results as they complete
+        std::lock_guard<std::mutex> lock(s->mu);
+        keep = s->cfg.keep_results;
+        s->cfg.keep_results = 0;
+    }
     auto t = sgb::serving::Clock::now();
     std::vector<int64_t> ids;
     for (int i = 0; i < n; ++i) {
@@ -579,7 +592,10 @@ extern "C" int sgemm_b200_server_run_poisson(sgemm_b200_server* srv, double rate
         ids.push_back(id);
     }
     const int d = sgemm_b200_server_drain(srv);
-    s->cfg.keep_results = keep;
+    {
+        std::lock_guard<std::mutex> lock(s->mu);
+        s->cfg.keep_results = keep;
+    }
     for (int64_t id : ids) sgemm_b200_server_release(srv, id);
     if (out) sgemm_b200_server_get_stats(srv, out);
     return d;
@@ -594,7 +610,10 @@ extern "C" void sgemm_b200_server_destroy(sgemm_b200_server* srv) {
         s->cv.notify_all();
     }
     if (s->worker.joinable()) s->worker.join();
-    cudaDeviceSynchronize();
+    // The server's own streams only; other work on the device is not waited for.
+    if (s->ingest) cudaStreamSynchronize(s->ingest);
+    for (auto& sl : s->slots)
+        if (sl.stream) cudaStreamSynchronize(sl.stream);
     for (auto& sl : s->slots) {
         sgb::grouped::arena_release(&sl.arena);
         if (sl.stream) cudaStreamDestroy(sl.stream);
