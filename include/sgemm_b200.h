@@ -221,7 +221,10 @@ int sgemm_b200_grouped_plan_create(sgemm_b200_grouped_plan** plan,
                                    const sgemm_b200_problem* problems, int count,
                                    const char* tuning_json);
 /* One persistent launch over every problem of the plan on `stream`.
- * use_graph != 0 replays a CUDA graph captured on the first call. */
+ * use_graph != 0 replays a CUDA graph captured on the first call.  A plan
+ * holds its own work-ticket counters, so launches of one plan must not
+ * overlap on the GPU: order them on one stream (distinct plans may run
+ * concurrently). */
 int sgemm_b200_grouped_plan_launch(sgemm_b200_grouped_plan* plan,
                                    sgemm_b200_stream_t stream, int use_graph);
 /* Tiles and work items in the plan's schedule (for tests and reports). */

@@ -599,21 +599,30 @@ static int launch(sgemm_b200_grouped_plan* plan, cudaStream_t stream, int use_gr
     if (!plan) return SGEMM_B200_ERR_INVALID_ARG;
     if (!use_graph) return enqueue(plan, stream);
     if (!plan->exec) {
-        cudaError_t e = cudaStreamCreateWithFlags(&plan->cap_stream, cudaStreamNonBlocking);
-        if (e != cudaSuccess) return cuda_status(e);
+        cudaError_t e = cudaSuccess;
+        if (!plan->cap_stream) {
+            e = cudaStreamCreateWithFlags(&plan->cap_stream, cudaStreamNonBlocking);
+            if (e != cudaSuccess) {
+                plan->cap_stream = nullptr;
+                return cuda_status(e);
+            }
+        }
         e = cudaStreamBeginCapture(plan->cap_stream, cudaStreamCaptureModeThreadLocal);
         if (e != cudaSuccess) return cuda_status(e);
         const int s = enqueue(plan, plan->cap_stream);
         cudaGraph_t graph = nullptr;
         e = cudaStreamEndCapture(plan->cap_stream, &graph);
-        if (s != SGEMM_B200_OK) {
+        if (s != SGEMM_B200_OK || e != cudaSuccess) {
             if (graph) cudaGraphDestroy(graph);
-            return s;
+            return s != SGEMM_B200_OK ? s : cuda_status(e);
         }
-        if (e != cudaSuccess) return cuda_status(e);
-        plan->graph = graph;
         e = cudaGraphInstantiate(&plan->exec, graph, 0);
-        if (e != cudaSuccess) return cuda_status(e);
+        if (e != cudaSuccess) {
+            plan->exec = nullptr;
+            cudaGraphDestroy(graph);
+            return cuda_status(e);
+        }
+        plan->graph = graph;
     }
     return cuda_status(cudaGraphLaunch(plan->exec, stream));
 }
