@@ -24,9 +24,11 @@
 //    autotuner (sgemm_b200_autotune_grouped), persisted as JSON keyed by the
 //    device name and SM count.
 #include <algorithm>
+#include <atomic>
 #include <cstdio>
 #include <cstring>
 #include <fstream>
+#include <mutex>
 #include <numeric>
 #include <sstream>
 #include <string>
@@ -495,11 +497,21 @@ static int make_schedule(const sgemm_b200_problem* probs, int count, const Table
     return SGEMM_B200_OK;
 }
 
+// The kernels' dynamic shared-memory attribute, once per device (attributes
+// belong to the device's context); a thread that sees the flag also sees the
+// attributes set.
 static void set_kernel_attributes() {
+    static std::atomic<bool> done[64];
+    static std::mutex mu;
+    const int dev = device_info().device;
+    if (dev < 0 || dev >= 64 || done[dev].load(std::memory_order_acquire)) return;
+    std::lock_guard<std::mutex> lock(mu);
+    if (done[dev].load(std::memory_order_relaxed)) return;
     cudaFuncSetAttribute(grouped_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          smem_bytes<3>());
     cudaFuncSetAttribute(grouped_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          smem_bytes<4>());
+    done[dev].store(true, std::memory_order_release);
 }
 
 // Persistent CTAs per SM of the kernel variant with `stages` stages.
@@ -693,11 +705,7 @@ int arena_launch(Arena* a, const sgemm_b200_problem* probs, int count, cudaStrea
                         cudaMemcpyHostToDevice, stream));
     chk(cudaMemsetAsync(a->d_counters, 0, sizeof(int) * n_counters, stream));
     if (e != cudaSuccess) return cuda_status(e);
-    static bool attrs = false;
-    if (!attrs) {
-        set_kernel_attributes();
-        attrs = true;
-    }
+    set_kernel_attributes();
     GParams p;
     p.probs = a->d_probs;
     p.items = a->d_items;

@@ -40,6 +40,7 @@
 // transposed to [split][N][Kp], both K-major) into a workspace.
 #include <cuda_bf16.h>
 
+#include <atomic>
 #include <cstring>
 #include <mutex>
 
@@ -502,12 +503,21 @@ static int launch(int m, int n, int k, float alpha, const float* A, int lda, con
     p.tiles_n = div_up(n, BN);
     p.vec_c = (ldc % 4 == 0) && (reinterpret_cast<uintptr_t>(C) % 16 == 0);
 
-    static bool attr_set[64] = {false};
+    // The kernel's shared-memory attribute, once per device; a thread that
+    // sees the flag also sees the attribute set.
+    static std::atomic<bool> attr_set[64];
+    static std::mutex attr_mu;
     const int dev = device_info().device;
-    if (dev >= 0 && dev < 64 && !attr_set[dev]) {
-        cudaFuncSetAttribute(split_gemm_kernel<PATH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             L::SMEM_BYTES);
-        attr_set[dev] = true;
+    if (dev < 0 || dev >= 64) return SGEMM_B200_ERR_CUDA;
+    if (!attr_set[dev].load(std::memory_order_acquire)) {
+        std::lock_guard<std::mutex> lock(attr_mu);
+        if (!attr_set[dev].load(std::memory_order_relaxed)) {
+            const cudaError_t e = cudaFuncSetAttribute(
+                split_gemm_kernel<PATH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                L::SMEM_BYTES);
+            if (e != cudaSuccess) return cuda_status(e);
+            attr_set[dev].store(true, std::memory_order_release);
+        }
     }
     split_gemm_kernel<PATH><<<p.tiles_m * p.tiles_n, THREADS, L::SMEM_BYTES, stream>>>(tmA, tmB,
                                                                                       p);
