@@ -18,6 +18,8 @@ by its own CUDA events with an L2-sized flush write in between steps.
                workload; the same leg checks the GPU rows bit for bit
   split        BF16x6 / TF32x3 tensor-core paths on the same 8192^3 problem,
                GFLOP/s and error against FP64 on sampled rows
+  config_1024  M=N=K=1024, alpha=1, beta=0: GFLOP/s, from host memory, and
+               the whole result checked bit for bit and against FP64
   split_configs  plain / BF16x6 / TF32x3 at 8192^3 and 16384^3 with entries
                sign * 2^e * U[1,2), GFLOP/s and FP64-checked error
   grouped, serving  the 512-problem grouped launch and the Poisson serving loop
@@ -290,15 +292,22 @@ def _cpu_baseline_and_checks(torch, sg, C_after, C0_host, size, checks, target_s
     ref, mag = oracle.dgemm(hA, hB, C0_host[sub], ALPHA, BETA, row_ids=sub)
     err = oracle.error_stats(C_after[sub], ref, mag)
     errors = {}
-    for label, n_size, dist, ids, outs in checks:
+    for chk in checks:
+        label, n_size, dist, ids, outs = chk[:5]
+        alpha, beta = chk[5] if len(chk) > 5 else (ALPHA, BETA)
+        exact_paths = chk[6] if len(chk) > 6 else ()
         hB_chk = hB if (n_size == size and dist == 0) else oracle.fill(n_size, n_size, SEED, 2,
                                                                         dist)
         a_rows = oracle.fill_rows(ids, n_size, SEED, 1, dist)
         c0_rows = oracle.fill_rows(ids, n_size, SEED, 3, dist)
-        ref_c, mag_c = oracle.dgemm(a_rows, hB_chk, c0_rows, ALPHA, BETA)
+        ref_c, mag_c = oracle.dgemm(a_rows, hB_chk, c0_rows, alpha, beta)
         errors[label] = {path: {k: float(v) for k, v in
                                 oracle.error_stats(rows_out, ref_c, mag_c).items()}
                          for path, rows_out in outs.items()}
+        for path in exact_paths:  # bit-for-bit against the kernel_basic restatement
+            want = oracle.sgemm_basic(a_rows, hB_chk, c0_rows, alpha, beta, basic=False)
+            errors[label][path]["bit_exact"] = int(np.sum(outs[path] == want))
+            errors[label][path]["elements"] = int(want.size)
     return {
         "value": round(gflops, 2), "unit": "GFLOP/s", "cores": threads, "kind": "port",
         "sample": f"{nrows} of {size} rows of the {size}^3 GEMM (C restatement of the "
@@ -354,6 +363,38 @@ def _split_leg(torch, sg, A, B, C0, flush, steps, warmup, rows, peaks, local):
         except Exception as e:  # report, never hide
             out[name] = {"error": str(e)}
     return out, samples
+
+
+def _config_1024_leg(torch, sg, steps, warmup):
+    """The smallest plain config: M=N=K=1024, alpha=1, beta=0, A and B
+    uniform[-1, 1) seed 0.  Device GFLOP/s, GFLOP/s from host memory through
+    sgemm_b200_host, and the whole result for the cpu_baseline leg's checks."""
+    n = 1024
+    A = torch.empty((n, n), device="cuda")
+    B = torch.empty_like(A)
+    C = torch.empty_like(A)
+    sg.fill_random(A, SEED, 1, sg.DIST_UNIFORM_PM1)
+    sg.fill_random(B, SEED, 2, sg.DIST_UNIFORM_PM1)
+    sg.fill_random(C, SEED, 3, sg.DIST_UNIFORM_PM1)  # never read: beta == 0
+    flush = torch.empty((256 << 20) // 4, device="cuda")
+    sg.sgemm(A, B, C, 1.0, 0.0)
+    torch.cuda.synchronize()
+    out = C.cpu().numpy()
+    ms = _time_steps(torch, lambda: sg.sgemm(A, B, C, 1.0, 0.0), steps, warmup, flush)
+    t = statistics.mean(ms)
+    hA, hB, hC = (X.cpu().pin_memory() for X in (A, B, C))
+
+    def host_step():
+        sg.sgemm_host(hA, hB, hC, 1.0, 0.0)
+
+    te = _time_steps(torch, host_step, steps, warmup, flush)
+    cfg = sg.config_names()[sg.select_config(n, n, n, A, n, B, n)]
+    res = {"gflops": round(2.0 * n ** 3 / (t * 1e-3) * 1e-9, 1), "ms_per_step": round(t, 4),
+           "e2e_gflops": round(2.0 * n ** 3 / (statistics.mean(te) * 1e-3) * 1e-9, 1),
+           "kernel_config": cfg, "alpha": 1.0, "beta": 0.0,
+           "dist": "uniform[-1,1) seed 0", "check": None}
+    ids = np.arange(n, dtype=np.int32)
+    return res, ("config_1024", n, 0, ids, {"plain": out}, (1.0, 0.0), ("plain",))
 
 
 def _split_configs_leg(torch, sg, sizes, steps, n_rows=32):
@@ -590,6 +631,9 @@ def run(args):
                              "ms_per_step": round(seq_ms, 3)}}
 
     checks = []
+    if rank == 0 and world == 1:
+        result["config_1024"], chk = _config_1024_leg(torch, sg, max(20, args.steps), args.warmup)
+        checks.append(chk)
     split_rows = np.linspace(0, SIZE - 1, 64).astype(np.int32)
     if rank == 0 and not args.skip_split:
         result["split"], samples = _split_leg(torch, sg, A, B, C0, flush,
@@ -612,6 +656,8 @@ def run(args):
                 result["split"][name]["error_vs_fp64_sampled_rows"] = uni[name]
         if "plain" in uni and "split" in result:
             result["split"]["plain_error_vs_fp64_same_rows"] = uni["plain"]
+        if "config_1024" in errors and "config_1024" in result:
+            result["config_1024"]["check"] = errors["config_1024"]["plain"]
         for label, errs in errors.items():
             if label.startswith("pow2_"):
                 for name, e in errs.items():
