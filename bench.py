@@ -257,6 +257,25 @@ def _e2e_host(torch, sg, steps, warmup, size):
     return ms, 3 * size * size * 4, size * size * 4, sg.host_plan(size, size, size)
 
 
+def _pcie_gbs(torch, nbytes=256 << 20, reps=5):
+    """Pinned host <-> device copy bandwidth (GB/s, best of reps): H2D, D2H."""
+    h = torch.empty(nbytes // 4, dtype=torch.float32, pin_memory=True)
+    d = torch.empty(nbytes // 4, device="cuda")
+    out = []
+    for dst, src in ((d, h), (h, d)):
+        best = 1e30
+        for _ in range(reps):
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record()
+            dst.copy_(src, non_blocking=True)
+            b.record()
+            torch.cuda.synchronize()
+            best = min(best, a.elapsed_time(b))
+        out.append(nbytes / (best * 1e-3) * 1e-9)
+    return out
+
+
 def _cpu_baseline_and_checks(torch, sg, C_after, C0_host, size, checks, target_s=10.0):
     """The CPU leg, where the oracle runs as the checker.  The oracle
     (kernel_basic restatement) on a bounded sample of rows of the same GEMM:
@@ -621,9 +640,17 @@ def run(args):
         ms_seq, _, _ = _e2e(torch, lambda a, b, c: sg.sgemm(a, b, c, ALPHA, BETA),
                             max(3, args.steps // 5), 2, SIZE)
         seq_ms = _max_over_ranks(dist, ms_seq)
+        h2d_gbs, d2h_gbs = _pcie_gbs(torch)
+        # the pipeline can be no faster than its slowest resource: the PCIe
+        # copies in either direction or the GEMM itself (device-timed above)
+        bound_ms = max(h2d / (h2d_gbs * 1e9) * 1e3, d2h / (d2h_gbs * 1e9) * 1e3, ms_step)
         result["e2e"] = {"value": round(flops * world / (e2e_ms * 1e-3) * 1e-9, 1),
                          "unit": "GFLOP/s", "ms_per_step": round(e2e_ms, 3),
                          "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                         "bound": {"ms": round(bound_ms, 3), "frac": round(bound_ms / e2e_ms, 4),
+                                   "h2d_gbs": round(h2d_gbs, 1), "d2h_gbs": round(d2h_gbs, 1),
+                                   "note": "max(H2D bytes / measured pinned H2D GB/s, D2H "
+                                           "bytes / measured D2H GB/s, device GEMM time)"},
                          "api": f"sgemm_b200_host, bands of {rows} rows x column chunks "
                                 f"{chunks}",
                          "copy_then_sgemm": {
