@@ -644,12 +644,15 @@ static int launch(sgemm_b200_grouped_plan* plan, cudaStream_t stream, int use_gr
 // buffers are allocated once and grown on demand, so a batch costs a host
 // schedule, a few async copies and one kernel launch (no cudaMalloc, no
 // graph capture).  An arena must not be reused before its previous batch
-// completed (the staging buffers feed async copies).
+// completed (the staging buffers feed async copies).  First allocations are
+// generous (min_cap elements), because growing pinned staging means
+// cudaFreeHost, which waits for the whole device, in the middle of serving.
 
 template <class T>
-static cudaError_t grow(T** d, T** h, size_t* cap, size_t need, cudaStream_t s) {
+static cudaError_t grow(T** d, T** h, size_t* cap, size_t need, cudaStream_t s,
+                        size_t min_cap) {
     if (need <= *cap) return cudaSuccess;
-    const size_t n = std::max(need, *cap * 2);
+    const size_t n = std::max({need, *cap * 2, min_cap});
     if (*d) cudaFreeAsync(*d, s);
     *d = nullptr;
     if (h && *h) {
@@ -676,11 +679,13 @@ int arena_launch(Arena* a, const sgemm_b200_problem* probs, int count, cudaStrea
         if (e == cudaSuccess) e = x;
     };
     const size_t n_counters = 1 + (size_t)sc.tickets;
-    chk(grow(&a->d_probs, &a->h_probs, &a->cap_probs, (size_t)count, stream));
-    chk(grow(&a->d_items, &a->h_items, &a->cap_items, sc.items.size(), stream));
-    chk(grow(&a->d_maps, &a->h_maps, &a->cap_maps, 2 * (size_t)count, stream));
-    chk(grow<int>(&a->d_counters, nullptr, &a->cap_counters, n_counters, stream));
-    chk(grow<float>(&a->d_ws, nullptr, &a->cap_ws, std::max<size_t>(sc.ws_floats, 1), stream));
+    // first capacities: 256 problems, 64 Ki work items (~1 MB pinned in all)
+    chk(grow(&a->d_probs, &a->h_probs, &a->cap_probs, (size_t)count, stream, 256));
+    chk(grow(&a->d_items, &a->h_items, &a->cap_items, sc.items.size(), stream, 1 << 16));
+    chk(grow(&a->d_maps, &a->h_maps, &a->cap_maps, 2 * (size_t)count, stream, 512));
+    chk(grow<int>(&a->d_counters, nullptr, &a->cap_counters, n_counters, stream, 1024));
+    chk(grow<float>(&a->d_ws, nullptr, &a->cap_ws, std::max<size_t>(sc.ws_floats, 1), stream,
+                    1));
     if (e != cudaSuccess) return cuda_status(e);
     std::memcpy(a->h_probs, sc.probs.data(), sizeof(GProblem) * count);
     std::memcpy(a->h_items, sc.items.data(), sizeof(GItem) * sc.items.size());
