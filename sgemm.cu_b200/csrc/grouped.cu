@@ -66,10 +66,13 @@ enum TileShape { kTileTall = 0, kTileWide = 1, kTileSkinny = 2 };  // 128x64, 64
 inline int tile_bm(int t) { return t == kTileTall ? 128 : t == kTileWide ? 64 : 32; }
 inline int tile_bn(int t) { return t == kTileTall ? 64 : 128; }
 
-// The 32 x 128 tile's throughput relative to the 8 x 8-thread tiles on work
-// that fills both; a problem takes it when its zero-padded area shrinks by
-// more than this factor.
-constexpr double kSkinnyEfficiency = 0.75;
+// Throughput of each tile relative to 128 x 64 on work that fills them
+// (measured on a B200 with the single-GEMM kernels of the same shapes).  A
+// problem leaves its bucket's tile for another when that tile's zero-padded
+// area divided by its efficiency is at least 2% smaller.
+inline double tile_efficiency(int t) {
+    return t == kTileTall ? 1.0 : t == kTileWide ? 0.994 : 0.75;
+}
 
 struct GProblem {
     Operands op;
@@ -455,13 +458,17 @@ static int make_schedule(const sgemm_b200_problem* probs, int count, const Table
         const Choice ch = table.c[bucket_of(q.m, q.n, q.k)];
         g.tile = ch.tile;
         {
-            // A problem a few rows tall runs on the 32 x 128 tile when that
-            // removes enough zero padding to pay for the narrower thread tile.
-            auto area = [&](int t) {
+            // Problem geometry: a problem a few rows tall (the 32 x 128 tile)
+            // or one whose edges fit the other 8 x 8 tile better loses less
+            // work to zero padding on that tile.
+            auto cost = [&](int t) {
                 return double(div_up(q.m, tile_bm(t)) * tile_bm(t)) *
-                       double(div_up(q.n, tile_bn(t)) * tile_bn(t));
+                       double(div_up(q.n, tile_bn(t)) * tile_bn(t)) / tile_efficiency(t);
             };
-            if (area(kTileSkinny) < kSkinnyEfficiency * area(ch.tile)) g.tile = kTileSkinny;
+            int best = ch.tile;
+            for (int t : {kTileTall, kTileWide, kTileSkinny})
+                if (cost(t) < 0.98 * cost(ch.tile) && cost(t) < cost(best)) best = t;
+            g.tile = best;
         }
         const int bm = tile_bm(g.tile), bn = tile_bn(g.tile);
         g.tma = tma_ok(q) ? 1 : 0;

@@ -15,16 +15,35 @@ def test_bucket_classes():
     assert sg.grouped_bucket(2048, 512, 100) == 6
 
 
+TILES = {"tall": (128, 64, 1.0), "wide": (64, 128, 0.994), "skinny": (32, 128, 0.75)}
+
+
+def _tile_for(m, n, bucket_tile="tall"):
+    """The library's per-problem rule: the bucket's tile unless another tile's
+    zero-padded area per unit efficiency is at least 2% smaller."""
+    def cost(t):
+        bm, bn, eff = TILES[t]
+        return math.ceil(m / bm) * bm * math.ceil(n / bn) * bn / eff
+    best = bucket_tile
+    for t in TILES:
+        if cost(t) < 0.98 * cost(bucket_tile) and cost(t) < cost(best):
+            best = t
+    return best
+
+
 def test_schedule_default_counts():
     shapes = [(64, 64, 64), (300, 520, 1001), (4096, 4096, 64), (1, 1, 1), (129, 257, 0)]
     probs = sg.host_problems(shapes)
     s = sg.grouped_schedule(probs)
     tiles = 0
-    for m, n, k in shapes:  # default tile: 128 x 64 for every bucket
-        tiles += math.ceil(m / 128) * math.ceil(n / 64)
+    for m, n, k in shapes:  # default bucket tile 128 x 64, adjusted per problem
+        bm, bn, _ = TILES[_tile_for(m, n)]
+        tiles += math.ceil(m / bm) * math.ceil(n / bn)
     assert s["tiles"] == tiles
     assert s["work_items"] == tiles  # no split-K by default: results equal the plain path
     assert s["workspace_bytes"] == 0
+    # the rule moves some of these off the default tile
+    assert [_tile_for(m, n) for m, n, _ in shapes] == ["tall", "wide", "tall", "skinny", "wide"]
 
 
 def test_schedule_ignores_table_for_other_device(tmp_path):
@@ -44,11 +63,16 @@ def test_schedule_rejects_bad_problem():
 
 
 def test_schedule_uses_skinny_tile_for_short_problems():
-    # problems a few rows tall run on 32 x 128 tiles instead of padding 128-row tiles
+    # problems a few rows tall run on 32 x 128 tiles instead of padding
+    # 128-row tiles; up to 64 rows the 64 x 128 tile is cheaper
     shapes = [(16, 4096, 4096), (1, 1000, 300), (33, 4100, 64), (48, 640, 2048)]
+    assert [_tile_for(m, n) for m, n, _ in shapes] == ["skinny", "skinny", "wide", "wide"]
     s = sg.grouped_schedule(sg.host_problems(shapes))
-    want = sum(math.ceil(m / 32) * math.ceil(n / 128) for m, n, k in shapes)
+    want = 0
+    for m, n, _ in shapes:
+        bm, bn, _ = TILES[_tile_for(m, n)]
+        want += math.ceil(m / bm) * math.ceil(n / bn)
     assert s["tiles"] == want
-    # square problems keep the 8 x 8-thread tiles
+    # square problems keep the 128 x 64 tile
     s = sg.grouped_schedule(sg.host_problems([(256, 256, 256)]))
     assert s["tiles"] == math.ceil(256 / 128) * math.ceil(256 / 64)
