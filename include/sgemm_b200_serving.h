@@ -19,8 +19,9 @@
  * the plain path's exact arithmetic per problem, and the split paths compute
  * each request alone.
  *
- * Latency of a request = completion (host callback after its batch) minus
- * submission, measured on the host's steady clock.
+ * Latency of a request = completion minus submission, on the host's steady
+ * clock.  Completion is when the server's completion thread, which polls an
+ * event recorded after each batch's last kernel, sees the batch finished.
  */
 #ifndef SGEMM_B200_SERVING_H
 #define SGEMM_B200_SERVING_H
@@ -57,7 +58,27 @@ typedef struct {
     double wall_s;
     size_t peak_pool_bytes;
     int64_t peak_waiting;          /* largest arrival-queue length seen */
+    /* latency split at the batch launch: queue = submission to the host-side
+     * launch of the request's batch, service = that launch to completion */
+    double queue_p50_ms, queue_p99_ms, service_p50_ms, service_p99_ms;
 } sgemm_b200_server_stats;
+
+/* One completed request.  Times are host steady-clock milliseconds from the
+ * first submission of the statistics window. */
+typedef struct {
+    int64_t request_id;
+    int m, n, k;
+    int batch_size;
+    int64_t batch;     /* batch number within the window, from 1 */
+    double submit_ms;  /* sgemm_b200_server_submit */
+    double admit_ms;   /* operands allocated from the pool, generation enqueued */
+    double launch_ms;  /* the batch's launch began on the host */
+    double done_ms;    /* the completion thread saw the batch finished */
+    /* the batch's span on the device (CUDA events after its operands are
+     * ready and after its last kernel), ms from an event recorded at the
+     * window's first submission; -1 when unavailable */
+    double device_start_ms, device_end_ms;
+} sgemm_b200_server_trace_record;
 
 int sgemm_b200_server_create(sgemm_b200_server** server, const sgemm_b200_server_config* cfg);
 void sgemm_b200_server_destroy(sgemm_b200_server* server);
@@ -80,6 +101,13 @@ int sgemm_b200_server_read_result(sgemm_b200_server* server, int64_t request_id,
 int sgemm_b200_server_release(sgemm_b200_server* server, int64_t request_id);
 
 int sgemm_b200_server_get_stats(sgemm_b200_server* server, sgemm_b200_server_stats* out);
+
+/* Copy the trace of the statistics window (run_poisson starts a new window):
+ * up to `max` records of completed requests in completion order; *count
+ * receives the number written.  A window keeps at most 1,048,576 records;
+ * later completions still count in the statistics but are not traced. */
+int sgemm_b200_server_get_trace(sgemm_b200_server* server, sgemm_b200_server_trace_record* out,
+                                int max, int* count);
 
 /* Open-loop load: `n_requests` requests with exponential inter-arrival times
  * of mean 1/rate_per_s; 60% tall-skinny (M uniform in [16, 256], N = K =

@@ -9,9 +9,14 @@
 //    fit in the pool (generating them on an ingest stream), forms a batch
 //    whenever one of `slots` streams is free, and launches it: one persistent
 //    grouped kernel (plain path) or one split GEMM per request (split paths),
-//    followed by a host callback;
-//  - the callback (a CUDA driver thread; it calls no CUDA API) stamps the
-//    completion time of the batch's requests and hands the slot back.
+//    followed by an event on the slot's stream;
+//  - one completion thread polls the events of the batches in flight
+//    (cudaEventQuery, about every 20 us, asleep while nothing is in flight),
+//    stamps the completion time of a finished batch's requests and hands the
+//    slot back.  Polling rather than a host callback (cudaLaunchHostFunc):
+//    on B200 the driver's callback thread was measured to start callbacks
+//    ~40 ms after their batch had finished on the device, once or twice per
+//    few thousand batches, which set the p99 of whole runs.
 // Requests that arrive while batches run are admitted as memory frees and
 // join the next batch; with two or more slots, batches overlap on the GPU.
 #include <algorithm>
@@ -46,6 +51,7 @@ namespace sgb {
 namespace serving {
 
 constexpr size_t kAlign = 256;
+constexpr size_t kMaxTrace = size_t(1) << 20;  // trace records kept per window
 
 static size_t round_up(size_t x) { return (x + kAlign - 1) / kAlign * kAlign; }
 
@@ -130,15 +136,18 @@ struct Request {
     int64_t off = -1;
     float *A = nullptr, *B = nullptr, *C = nullptr;
     void* ws = nullptr;
-    double t_submit = 0, t_done = 0;
+    double t_submit = 0, t_admit = 0, t_launch = 0, t_done = 0;
     int state = kWaiting;
     int batch_size = 0;
+    int64_t batch = 0;
     bool auto_release = false;
     cudaEvent_t ready = nullptr;
 };
 
 struct Slot {
     cudaStream_t stream = nullptr;
+    cudaEvent_t ev_start = nullptr, ev_end = nullptr;  // device span of the current batch
+    bool error = false;  // the batch's end event reported an error
     bool busy = false;
     std::vector<Request*> batch;
     grouped::Arena arena;
@@ -146,34 +155,32 @@ struct Slot {
 
 struct Server;
 
-struct DoneCtx {
-    Server* server;
-    int slot;
-};
-
 struct Server {
     sgemm_b200_server_config cfg;
     uint8_t* d_pool = nullptr;
     sgemm_b200_pool pool;
     cudaStream_t ingest = nullptr;
+    cudaEvent_t epoch = nullptr;  // recorded on `ingest` at the window's first submission
+    bool epoch_set = false;
     std::vector<Slot> slots;
-    std::vector<DoneCtx> ctx;
+    std::vector<int> polling;  // slots whose batch is on the GPU, oldest first
     int device = 0;
 
     std::mutex mu;
-    std::condition_variable cv, cv_drain;
+    std::condition_variable cv, cv_drain, cv_poll;
     std::deque<Request*> arrivals;
     std::deque<Request*> ready;
     std::deque<int> finished_slots;
     std::unordered_map<int64_t, Request*> all;
-    std::thread worker;
+    std::thread worker, completer;
     bool stop = false;
     int64_t next_id = 1;
     int64_t outstanding = 0;  // submitted and not yet done / rejected / failed
     int64_t admissions = 0;
 
     // stats
-    std::vector<double> latencies_ms;
+    std::vector<double> latencies_ms, queue_ms, service_ms;
+    std::vector<sgemm_b200_server_trace_record> trace;
     double flops_done = 0, t_first_submit = -1, t_last_done = 0;
     int64_t submitted = 0, completed = 0, rejected = 0, failed = 0, batches = 0;
     int in_flight = 0, max_in_flight = 0, max_batch_seen = 0;
@@ -181,14 +188,43 @@ struct Server {
     int64_t peak_waiting = 0;
 };
 
-static void CUDART_CB on_batch_done(void* p) {
-    DoneCtx* c = static_cast<DoneCtx*>(p);
-    Server* s = c->server;
-    const double t = secs(Clock::now());
-    std::lock_guard<std::mutex> lock(s->mu);
-    for (Request* r : s->slots[c->slot].batch) r->t_done = t;
-    s->finished_slots.push_back(c->slot);
-    s->cv.notify_all();
+// Completion thread: polls the end events of the batches in flight.
+static void completer_loop(Server* s) {
+    cudaSetDevice(s->device);
+    std::unique_lock<std::mutex> lock(s->mu);
+    while (true) {
+        if (s->polling.empty()) {
+            if (s->stop && s->outstanding == 0) break;
+            s->cv_poll.wait_for(lock, std::chrono::milliseconds(50));
+            continue;
+        }
+        const std::vector<int> slots = s->polling;
+        lock.unlock();
+        std::vector<int> done;
+        std::vector<bool> ok;
+        for (int si : slots) {
+            const cudaError_t q = cudaEventQuery(s->slots[si].ev_end);
+            if (q == cudaErrorNotReady) continue;
+            done.push_back(si);
+            ok.push_back(q == cudaSuccess);
+        }
+        const double t = secs(Clock::now());
+        lock.lock();
+        for (size_t i = 0; i < done.size(); ++i) {
+            const int si = done[i];
+            s->slots[si].error = !ok[i];
+            for (Request* r : s->slots[si].batch) r->t_done = t;
+            s->polling.erase(std::find(s->polling.begin(), s->polling.end(), si));
+            s->finished_slots.push_back(si);
+        }
+        if (!done.empty()) {
+            s->cv.notify_all();
+            continue;
+        }
+        lock.unlock();
+        std::this_thread::sleep_for(std::chrono::microseconds(20));
+        lock.lock();
+    }
 }
 
 static size_t request_bytes(int path, int m, int n, int k, size_t* ws) {
@@ -202,17 +238,43 @@ static size_t request_bytes(int path, int m, int n, int k, size_t* ws) {
 // Called with the lock held.
 static void finish_slot(Server* s, int si) {
     Slot& sl = s->slots[si];
+    // the batch's device span on the device clock, from the window's epoch
+    float g0 = -1.f, g1 = -1.f;
+    if (s->epoch_set && (cudaEventElapsedTime(&g0, s->epoch, sl.ev_start) != cudaSuccess ||
+                         cudaEventElapsedTime(&g1, s->epoch, sl.ev_end) != cudaSuccess)) {
+        g0 = g1 = -1.f;
+        cudaGetLastError();  // a failed query must not surface at this thread's next launch
+    }
     for (Request* r : sl.batch) {
-        r->state = kDone;
-        s->latencies_ms.push_back((r->t_done - r->t_submit) * 1e3);
-        s->flops_done += 2.0 * r->m * (double)r->n * r->k;
-        s->t_last_done = std::max(s->t_last_done, r->t_done);
-        ++s->completed;
-        --s->outstanding;
         if (r->ready) {
             cudaEventDestroy(r->ready);
             r->ready = nullptr;
         }
+        if (sl.error) {  // the device reported an error for the batch
+            r->state = kFailed;
+            ++s->failed;
+            --s->outstanding;
+            if (r->auto_release) {
+                pool_free(&s->pool, r->off);
+                r->off = -1;
+            }
+            continue;
+        }
+        r->state = kDone;
+        s->latencies_ms.push_back((r->t_done - r->t_submit) * 1e3);
+        s->queue_ms.push_back((r->t_launch - r->t_submit) * 1e3);
+        s->service_ms.push_back((r->t_done - r->t_launch) * 1e3);
+        if (s->trace.size() < kMaxTrace) {
+            const double t0 = s->t_first_submit;
+            s->trace.push_back(sgemm_b200_server_trace_record{
+                r->id, r->m, r->n, r->k, r->batch_size, r->batch, (r->t_submit - t0) * 1e3,
+                (r->t_admit - t0) * 1e3, (r->t_launch - t0) * 1e3, (r->t_done - t0) * 1e3,
+                (double)g0, (double)g1});
+        }
+        s->flops_done += 2.0 * r->m * (double)r->n * r->k;
+        s->t_last_done = std::max(s->t_last_done, r->t_done);
+        ++s->completed;
+        --s->outstanding;
         if (r->auto_release) {
             pool_free(&s->pool, r->off);
             r->off = -1;
@@ -220,6 +282,7 @@ static void finish_slot(Server* s, int si) {
     }
     sl.batch.clear();
     sl.busy = false;
+    sl.error = false;
     --s->in_flight;
 }
 
@@ -261,6 +324,7 @@ static void admit(Server* s) {
                                s->ingest);
         cudaEventCreateWithFlags(&r->ready, cudaEventDisableTiming);
         cudaEventRecord(r->ready, s->ingest);
+        r->t_admit = secs(Clock::now());
         r->state = kAdmitted;
         s->ready.push_back(r);
     }
@@ -271,8 +335,8 @@ static int launch_batch(Server* s, int si) {
     if (s->cfg.inject_batch_delay_ms > 0)
         std::this_thread::sleep_for(std::chrono::milliseconds(s->cfg.inject_batch_delay_ms));
     for (Request* r : sl.batch) cudaStreamWaitEvent(sl.stream, r->ready, 0);
-    int st = SGEMM_B200_OK;
-    if (s->cfg.path == SGEMM_B200_PATH_PLAIN) {
+    int st = cuda_status(cudaEventRecord(sl.ev_start, sl.stream));
+    if (st == SGEMM_B200_OK && s->cfg.path == SGEMM_B200_PATH_PLAIN) {
         std::vector<sgemm_b200_problem> probs(sl.batch.size());
         for (size_t i = 0; i < sl.batch.size(); ++i) {
             const Request* r = sl.batch[i];
@@ -280,15 +344,14 @@ static int launch_batch(Server* s, int si) {
                                           r->beta, r->A, r->B, r->C};
         }
         st = grouped::arena_launch(&sl.arena, probs.data(), (int)probs.size(), sl.stream);
-    } else {
+    } else if (st == SGEMM_B200_OK) {
         for (Request* r : sl.batch) {
             st = sgemm_b200_split(s->cfg.path, r->m, r->n, r->k, &r->alpha, r->A, r->k, r->B,
                                   r->n, &r->beta, r->C, r->n, r->ws, r->ws_bytes, sl.stream);
             if (st != SGEMM_B200_OK) break;
         }
     }
-    if (st == SGEMM_B200_OK)
-        st = cuda_status(cudaLaunchHostFunc(sl.stream, on_batch_done, &s->ctx[si]));
+    if (st == SGEMM_B200_OK) st = cuda_status(cudaEventRecord(sl.ev_end, sl.stream));
     return st;
 }
 
@@ -317,10 +380,15 @@ static void worker_loop(Server* s) {
                 r->state = kRunning;
                 sl.batch.push_back(r);
             }
-            for (Request* r : sl.batch) r->batch_size = (int)sl.batch.size();
             sl.busy = true;
             ++s->in_flight;
             ++s->batches;
+            const double t_launch = secs(Clock::now());
+            for (Request* r : sl.batch) {
+                r->batch_size = (int)sl.batch.size();
+                r->batch = s->batches;
+                r->t_launch = t_launch;
+            }
             s->max_in_flight = std::max(s->max_in_flight, s->in_flight);
             s->max_batch_seen = std::max(s->max_batch_seen, (int)sl.batch.size());
             lock.unlock();
@@ -348,6 +416,9 @@ static void worker_loop(Server* s) {
                 sl.batch.clear();
                 sl.busy = false;
                 --s->in_flight;
+            } else {
+                s->polling.push_back(free_slot);
+                s->cv_poll.notify_one();
             }
             continue;
         }
@@ -409,21 +480,27 @@ extern "C" int sgemm_b200_server_create(sgemm_b200_server** out,
     s->pool.free_[0] = s->pool.capacity;
     cudaError_t e = cudaMalloc(&s->d_pool, s->pool.capacity);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->ingest, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreate(&s->epoch);
     s->slots.resize(cfg->slots);
-    s->ctx.resize(cfg->slots);
     for (int i = 0; i < cfg->slots && e == cudaSuccess; ++i) {
         e = cudaStreamCreateWithFlags(&s->slots[i].stream, cudaStreamNonBlocking);
-        s->ctx[i] = sgb::serving::DoneCtx{s, i};
+        if (e == cudaSuccess) e = cudaEventCreate(&s->slots[i].ev_start);
+        if (e == cudaSuccess) e = cudaEventCreate(&s->slots[i].ev_end);
     }
     if (e != cudaSuccess) {
-        for (auto& sl : s->slots)
+        for (auto& sl : s->slots) {
             if (sl.stream) cudaStreamDestroy(sl.stream);
+            if (sl.ev_start) cudaEventDestroy(sl.ev_start);
+            if (sl.ev_end) cudaEventDestroy(sl.ev_end);
+        }
+        if (s->epoch) cudaEventDestroy(s->epoch);
         if (s->ingest) cudaStreamDestroy(s->ingest);
         cudaFree(s->d_pool);
         delete srv;
         return sgb::cuda_status(e);
     }
     s->worker = std::thread(sgb::serving::worker_loop, s);
+    s->completer = std::thread(sgb::serving::completer_loop, s);
     *out = srv;
     return SGEMM_B200_OK;
 }
@@ -447,7 +524,10 @@ extern "C" int sgemm_b200_server_submit(sgemm_b200_server* srv, int m, int n, in
     s->all[r->id] = r;
     if (id) *id = r->id;
     ++s->submitted;
-    if (s->t_first_submit < 0) s->t_first_submit = r->t_submit;
+    if (s->t_first_submit < 0) {
+        s->t_first_submit = r->t_submit;
+        s->epoch_set = cudaEventRecord(s->epoch, s->ingest) == cudaSuccess;
+    }
     if (r->bytes > s->pool.capacity) {  // could never fit: refuse now
         r->state = sgb::serving::kRejected;
         ++s->rejected;
@@ -533,25 +613,44 @@ extern "C" int sgemm_b200_server_get_stats(sgemm_b200_server* srv, sgemm_b200_se
     st.batches = s->batches;
     st.max_batches_in_flight = s->max_in_flight;
     st.max_batch_size = s->max_batch_seen;
-    std::vector<double> l = s->latencies_ms;
+    // nearest-rank percentile of a sorted sample
+    auto pct = [](const std::vector<double>& v, double q) {
+        const size_t i = std::min(v.size() - 1, (size_t)std::ceil(q * v.size()) - 1);
+        return v[i];
+    };
+    std::vector<double> l = s->latencies_ms, qu = s->queue_ms, sv = s->service_ms;
     std::sort(l.begin(), l.end());
+    std::sort(qu.begin(), qu.end());
+    std::sort(sv.begin(), sv.end());
     if (!l.empty()) {
-        auto pct = [&](double q) {
-            const size_t i = std::min(l.size() - 1, (size_t)std::ceil(q * l.size()) - 1);
-            return l[i];
-        };
-        st.p50_ms = pct(0.50);
-        st.p99_ms = pct(0.99);
+        st.p50_ms = pct(l, 0.50);
+        st.p99_ms = pct(l, 0.99);
         double sum = 0;
         for (double v : l) sum += v;
         st.mean_ms = sum / l.size();
         st.max_ms = l.back();
+        st.queue_p50_ms = pct(qu, 0.50);
+        st.queue_p99_ms = pct(qu, 0.99);
+        st.service_p50_ms = pct(sv, 0.50);
+        st.service_p99_ms = pct(sv, 0.99);
     }
     st.wall_s = s->t_first_submit >= 0 ? s->t_last_done - s->t_first_submit : 0;
     st.gflops = st.wall_s > 0 ? s->flops_done / st.wall_s * 1e-9 : 0;
     st.peak_pool_bytes = s->peak_pool;
     st.peak_waiting = s->peak_waiting;
     *out = st;
+    return SGEMM_B200_OK;
+}
+
+extern "C" int sgemm_b200_server_get_trace(sgemm_b200_server* srv,
+                                           sgemm_b200_server_trace_record* out, int max,
+                                           int* count) {
+    if (!srv || !count || max < 0 || (max > 0 && !out)) return SGEMM_B200_ERR_INVALID_ARG;
+    Server* s = &srv->s;
+    std::lock_guard<std::mutex> lock(s->mu);
+    const int n = (int)std::min<size_t>(s->trace.size(), (size_t)max);
+    std::copy(s->trace.begin(), s->trace.begin() + n, out);
+    *count = n;
     return SGEMM_B200_OK;
 }
 
@@ -566,8 +665,12 @@ extern "C" int sgemm_b200_server_run_poisson(sgemm_b200_server* srv, double rate
         // this run's statistics start fresh
         std::lock_guard<std::mutex> lock(s->mu);
         s->latencies_ms.clear();
+        s->queue_ms.clear();
+        s->service_ms.clear();
+        s->trace.clear();
         s->flops_done = 0;
         s->t_first_submit = -1;
+        s->epoch_set = false;
         s->t_last_done = 0;
         s->submitted = s->completed = s->rejected = s->failed = s->batches = 0;
         s->max_in_flight = s->max_batch_seen = 0;
@@ -609,7 +712,9 @@ extern "C" void sgemm_b200_server_destroy(sgemm_b200_server* srv) {
         s->stop = true;
         s->cv.notify_all();
     }
+    s->cv_poll.notify_all();
     if (s->worker.joinable()) s->worker.join();
+    if (s->completer.joinable()) s->completer.join();
     // The server's own streams only; other work on the device is not waited for.
     if (s->ingest) cudaStreamSynchronize(s->ingest);
     for (auto& sl : s->slots)
@@ -617,7 +722,10 @@ extern "C" void sgemm_b200_server_destroy(sgemm_b200_server* srv) {
     for (auto& sl : s->slots) {
         sgb::grouped::arena_release(&sl.arena);
         if (sl.stream) cudaStreamDestroy(sl.stream);
+        if (sl.ev_start) cudaEventDestroy(sl.ev_start);
+        if (sl.ev_end) cudaEventDestroy(sl.ev_end);
     }
+    if (s->epoch) cudaEventDestroy(s->epoch);
     if (s->ingest) cudaStreamDestroy(s->ingest);
     for (auto& kv : s->all) {
         if (kv.second->ready) cudaEventDestroy(kv.second->ready);

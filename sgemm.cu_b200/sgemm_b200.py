@@ -75,10 +75,24 @@ class ServerStats(ctypes.Structure):
         ("p50_ms", ctypes.c_double), ("p99_ms", ctypes.c_double), ("mean_ms", ctypes.c_double),
         ("max_ms", ctypes.c_double), ("gflops", ctypes.c_double), ("wall_s", ctypes.c_double),
         ("peak_pool_bytes", ctypes.c_size_t), ("peak_waiting", ctypes.c_int64),
+        ("queue_p50_ms", ctypes.c_double), ("queue_p99_ms", ctypes.c_double),
+        ("service_p50_ms", ctypes.c_double), ("service_p99_ms", ctypes.c_double),
     ]
 
     def as_dict(self) -> dict:
         return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+class TraceRecord(ctypes.Structure):
+    """Mirror of sgemm_b200_server_trace_record."""
+
+    _fields_ = [
+        ("request_id", ctypes.c_int64), ("m", ctypes.c_int), ("n", ctypes.c_int),
+        ("k", ctypes.c_int), ("batch_size", ctypes.c_int), ("batch", ctypes.c_int64),
+        ("submit_ms", ctypes.c_double), ("admit_ms", ctypes.c_double),
+        ("launch_ms", ctypes.c_double), ("done_ms", ctypes.c_double),
+        ("device_start_ms", ctypes.c_double), ("device_end_ms", ctypes.c_double),
+    ]
 
 
 _lib: Optional[ctypes.CDLL] = None
@@ -139,6 +153,8 @@ def _declare(lib: ctypes.CDLL) -> None:
     d("sgemm_b200_server_read_result", _I, [_P, ctypes.c_int64, ctypes.c_void_p])
     d("sgemm_b200_server_release", _I, [_P, ctypes.c_int64])
     d("sgemm_b200_server_get_stats", _I, [_P, ctypes.POINTER(ServerStats)])
+    d("sgemm_b200_server_get_trace", _I, [_P, ctypes.POINTER(TraceRecord), _I,
+                                          ctypes.POINTER(ctypes.c_int)])
     d("sgemm_b200_server_run_poisson", _I, [_P, ctypes.c_double, _I, ctypes.c_uint64,
                                            ctypes.POINTER(ServerStats)])
     d("sgemm_b200_serving_workload", _I, [_I, ctypes.c_double, ctypes.c_uint64,
@@ -435,6 +451,17 @@ class Server:
         st = ServerStats()
         _check(lib().sgemm_b200_server_get_stats(self._h, ctypes.byref(st)), "stats")
         return st.as_dict()
+
+    def trace(self) -> list:
+        """Completed requests of the statistics window, in completion order:
+        one dict per request with times in ms from its first submission."""
+        cap = int(self.stats()["completed"])
+        buf = (TraceRecord * max(cap, 1))()
+        count = ctypes.c_int(0)
+        _check(lib().sgemm_b200_server_get_trace(self._h, buf, cap, ctypes.byref(count)),
+               "trace")
+        return [{name: getattr(buf[i], name) for name, _ in TraceRecord._fields_}
+                for i in range(count.value)]
 
     def run_poisson(self, rate_per_s: float, n_requests: int, seed: int = 0) -> dict:
         st = ServerStats()

@@ -122,3 +122,36 @@ def test_selftest_wait_validation():
     assert sg.lib().sgemm_b200_selftest_wait_timeout(0, None) == sg.ERR_INVALID_ARG
     assert sg.lib().sgemm_b200_selftest_wait_timeout(-5, None) == sg.ERR_INVALID_ARG
     assert sg.lib().sgemm_b200_selftest_wait_timeout(10000001, None) == sg.ERR_INVALID_ARG
+
+
+@pytest.mark.parametrize("mirror,c_name,header", [
+    (sg.Problem, "sgemm_b200_problem", "sgemm_b200.h"),
+    (sg.ServerConfig, "sgemm_b200_server_config", "sgemm_b200_serving.h"),
+    (sg.ServerStats, "sgemm_b200_server_stats", "sgemm_b200_serving.h"),
+    (sg.TraceRecord, "sgemm_b200_server_trace_record", "sgemm_b200_serving.h"),
+])
+def test_ctypes_mirrors_match_the_c_layout(mirror, c_name, header, tmp_path):
+    # compile a probe against the public header and compare size and every
+    # field offset with the ctypes mirror
+    import shutil
+    import subprocess
+    if shutil.which("gcc") is None:
+        pytest.skip("no C compiler")
+    fields = [name for name, _ in mirror._fields_]
+    src = tmp_path / "layout.c"
+    src.write_text(
+        "#include <stdio.h>\n#include <stddef.h>\n"
+        f'#include "{header}"\n'
+        "int main(void) {\n"
+        f'  printf("%zu\\n", sizeof({c_name}));\n'
+        + "".join(f'  printf("%zu\\n", offsetof({c_name}, {f}));\n' for f in fields)
+        + "  return 0;\n}\n")
+    exe = tmp_path / "layout"
+    cuda_inc = os.path.join(os.environ.get("CUDA_HOME", "/usr/local/cuda"), "include")
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), "-I", cuda_inc, str(src), "-o",
+                    str(exe)], check=True)
+    got = [int(x) for x in subprocess.run([str(exe)], check=True, capture_output=True,
+                                          text=True).stdout.split()]
+    assert got[0] == ctypes.sizeof(mirror)
+    for f, off in zip(fields, got[1:]):
+        assert off == getattr(mirror, f).offset, f

@@ -103,3 +103,39 @@ def test_injected_allocation_failures_and_delays():
     print(st)
     assert st["failed"] == 3 and st["completed"] == 6
     assert st["p50_ms"] >= 20.0  # every batch waited the injected delay
+
+
+@pytest.mark.parametrize("path", ["plain", "bf16x6"])
+def test_trace_accounts_for_every_request(path):
+    srv = sg.Server(64 << 30, slots=2, max_batch=16, path=path)
+    st = srv.run_poisson(rate_per_s=2000.0, n_requests=120, seed=9)
+    tr = srv.trace()
+    srv.close()
+    assert st["completed"] == 120 and len(tr) == 120
+    assert len({r["request_id"] for r in tr}) == 120
+    eps = 1e-9
+    for r in tr:
+        assert -eps <= r["submit_ms"] <= r["admit_ms"] + eps
+        assert r["admit_ms"] <= r["launch_ms"] + eps <= r["done_ms"] + 2 * eps
+        # device span: after the window's epoch, ends before the host hears of
+        # it (the host and device axes differ by the epoch's enqueue delay)
+        assert 0.0 <= r["device_start_ms"] <= r["device_end_ms"]
+        assert r["device_end_ms"] <= r["done_ms"] + 0.5
+    # every batch's records: all of its requests, one launch and one completion
+    by_batch = {}
+    for r in tr:
+        by_batch.setdefault(r["batch"], []).append(r)
+    assert len(by_batch) == st["batches"]
+    for recs in by_batch.values():
+        assert len(recs) == recs[0]["batch_size"]
+        assert len({r["launch_ms"] for r in recs}) == 1 and len({r["done_ms"] for r in recs}) == 1
+    # the statistics are the trace's percentiles (nearest rank)
+    def pct(v, q):
+        v = sorted(v)
+        return v[min(len(v) - 1, int(np.ceil(q * len(v))) - 1)]
+    lat = [r["done_ms"] - r["submit_ms"] for r in tr]
+    que = [r["launch_ms"] - r["submit_ms"] for r in tr]
+    svc = [r["done_ms"] - r["launch_ms"] for r in tr]
+    assert pct(lat, 0.99) == pytest.approx(st["p99_ms"], abs=1e-6)
+    assert pct(que, 0.99) == pytest.approx(st["queue_p99_ms"], abs=1e-6)
+    assert pct(svc, 0.50) == pytest.approx(st["service_p50_ms"], abs=1e-6)
