@@ -198,6 +198,20 @@ int sgemm_b200_host(int path, int m, int n, int k,
 int sgemm_b200_host_plan(int path, int m, int n, int k, int reads_c, int* rows,
                          int* chunk_cols, int max_chunks);
 
+/* sgemm_b200_host with the caller's block plan instead of the built-in one:
+ * bands of `rows` rows (the last takes the rest; at most 16 bands) times
+ * `nchunks` (1..4) column chunks of the widths in chunk_cols, which must sum
+ * to n.  Same result, bit for bit, for every valid plan; an invalid plan
+ * returns SGEMM_B200_ERR_INVALID_ARG before any work. */
+int sgemm_b200_host_planned(int path, int m, int n, int k,
+                            const float* alpha,
+                            const float* A, int lda,
+                            const float* B, int ldb,
+                            const float* beta,
+                            float* C, int ldc,
+                            int rows, const int* chunk_cols, int nchunks,
+                            sgemm_b200_stream_t stream);
+
 /* ------------------------------------------------------------------------ */
 /* Grouped persistent GEMM (no reference counterpart)                        */
 /* ------------------------------------------------------------------------ */

@@ -176,16 +176,29 @@ Plan make_plan(int path, int m, int n, int k, bool read_c) {
     return best;
 }
 
+// A plan is usable when its chunks cover n, its bands number at most
+// kMaxBands and its blocks at most kMaxBlocks (the engine's event arrays).
+static bool plan_ok(const Plan& p, int m, int n) {
+    if (p.rows < 1 || p.nchunks < 1 || p.nchunks > kMaxChunks) return false;
+    if ((m + p.rows - 1) / p.rows > kMaxBands) return false;
+    long long cols = 0;
+    for (int j = 0; j < p.nchunks; ++j) {
+        if (p.cols[j] < 1) return false;
+        cols += p.cols[j];
+    }
+    return cols == n;
+}
+
 static int run(int path, int m, int n, int k, const float* alpha, const float* A, int lda,
                const float* B, int ldb, const float* beta, float* C, int ldc,
-               cudaStream_t stream) {
+               cudaStream_t stream, const Plan* forced) {
     Engine* eng = engine();
     if (!eng) return SGEMM_B200_ERR_CUDA;
     cudaMemPool_t pool = library_pool();
     if (!pool) return SGEMM_B200_ERR_CUDA;
 
     const bool read_c = *beta != 0.0f;  // beta == 0: C is written, never read
-    const Plan plan = make_plan(path, m, n, k, read_c);
+    const Plan plan = forced ? *forced : make_plan(path, m, n, k, read_c);
     const int bands = (m + plan.rows - 1) / plan.rows;
     // Device pitches: rows start on 16 bytes, so the TMA kernels take every block.
     const int lda_d = (k + 3) / 4 * 4, ldb_d = (n + 3) / 4 * 4, ldc_d = (n + 3) / 4 * 4;
@@ -278,7 +291,36 @@ extern "C" int sgemm_b200_host(int path, int m, int n, int k, const float* alpha
             s = SGEMM_B200_ERR_UNSUPPORTED;
         else
             s = sgb::host::run(path, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc,
-                               sgb::as_stream(stream));
+                               sgb::as_stream(stream), nullptr);
+    }
+    sgb::set_last_status(s);
+    return s;
+}
+
+extern "C" int sgemm_b200_host_planned(int path, int m, int n, int k, const float* alpha,
+                                       const float* A, int lda, const float* B, int ldb,
+                                       const float* beta, float* C, int ldc, int rows,
+                                       const int* chunk_cols, int nchunks,
+                                       sgemm_b200_stream_t stream) {
+    int s = sgb::check_gemm_args(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+    if (s == SGEMM_B200_OK && path != SGEMM_B200_PATH_PLAIN && path != SGEMM_B200_PATH_BF16X6 &&
+        path != SGEMM_B200_PATH_TF32X3)
+        s = SGEMM_B200_ERR_INVALID_ARG;
+    sgb::host::Plan p{rows, nchunks, {}};
+    if (s == SGEMM_B200_OK && m > 0 && n > 0) {
+        if (!chunk_cols || nchunks < 1 || nchunks > sgb::host::kMaxChunks) {
+            s = SGEMM_B200_ERR_INVALID_ARG;
+        } else {
+            for (int j = 0; j < nchunks; ++j) p.cols[j] = chunk_cols[j];
+            if (!sgb::host::plan_ok(p, m, n)) s = SGEMM_B200_ERR_INVALID_ARG;
+        }
+    }
+    if (s == SGEMM_B200_OK && m > 0 && n > 0) {
+        if (!sgb::device_is_sm100())
+            s = SGEMM_B200_ERR_UNSUPPORTED;
+        else
+            s = sgb::host::run(path, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc,
+                               sgb::as_stream(stream), &p);
     }
     sgb::set_last_status(s);
     return s;

@@ -121,6 +121,7 @@ def _declare(lib: ctypes.CDLL) -> None:
     d("sgemm_b200_host", _I, [_I] + _GEMM_ARGS + [_P])
     d("sgemm_b200_host_plan", _I, [_I, _I, _I, _I, _I, ctypes.POINTER(_I), ctypes.POINTER(_I),
                                    _I])
+    d("sgemm_b200_host_planned", _I, [_I] + _GEMM_ARGS + [_I, ctypes.POINTER(_I), _I, _P])
     d("sgemm_b200_grouped_plan_create", _I,
       [ctypes.POINTER(_P), ctypes.POINTER(Problem), _I, ctypes.c_char_p])
     d("sgemm_b200_grouped_plan_launch", _I, [_P, _P, _I])
@@ -270,10 +271,11 @@ def gemm(path, A, B, C, alpha: float = 1.0, beta: float = 0.0, stream=None) -> N
 
 
 def sgemm_host(A, B, C, alpha: float = 1.0, beta: float = 0.0, path="plain",
-               stream=None) -> None:
+               stream=None, plan=None) -> None:
     """C := alpha*A@B + beta*C with A, B, C in HOST memory (CPU tensors, ideally
     pinned): the library stages blocks of C through HBM with the copies
-    overlapping the kernels, and writes C back in place."""
+    overlapping the kernels, and writes C back in place.  `plan` = (rows per
+    band, [column chunk widths]) replaces the built-in block plan."""
     p = PATHS[path] if isinstance(path, str) else int(path)
     m, k = A.shape
     k2, n = B.shape
@@ -282,8 +284,15 @@ def sgemm_host(A, B, C, alpha: float = 1.0, beta: float = 0.0, path="plain",
     pa, lda = _mat(A, "A", "cpu")
     pb, ldb = _mat(B, "B", "cpu")
     pc, ldc = _mat(C, "C", "cpu")
-    _check(lib().sgemm_b200_host(p, m, n, k, _f(alpha), pa, lda, pb, ldb, _f(beta), pc, ldc,
-                                 _stream_ptr(stream)), "sgemm_b200_host")
+    if plan is None:
+        _check(lib().sgemm_b200_host(p, m, n, k, _f(alpha), pa, lda, pb, ldb, _f(beta), pc, ldc,
+                                     _stream_ptr(stream)), "sgemm_b200_host")
+        return
+    rows, widths = plan
+    cols = (ctypes.c_int * max(1, len(widths)))(*widths)
+    _check(lib().sgemm_b200_host_planned(p, m, n, k, _f(alpha), pa, lda, pb, ldb, _f(beta), pc,
+                                         ldc, int(rows), cols, len(widths),
+                                         _stream_ptr(stream)), "sgemm_b200_host_planned")
 
 
 def host_plan(m: int, n: int, k: int, reads_c: bool = True, path="plain") -> tuple:

@@ -117,6 +117,26 @@ def test_host_entry_validation_and_bands():
             assert all(c % 128 == 0 and c >= 512 for c in chunks[:-1])
             assert len(chunks) == 1 or chunks[-1] >= 512
 
+def test_host_planned_rejects_invalid_plans():
+    # plan checks run before any device work (pointers are never touched)
+    l = sg.lib()
+    a = ctypes.c_float(1.0)
+    b = ctypes.c_float(0.5)
+
+    def call(rows, widths, m=1000, n=600):
+        cols = (ctypes.c_int * max(1, len(widths)))(*widths)
+        return l.sgemm_b200_host_planned(0, m, n, 64, ctypes.byref(a), 16, 64, 16, n,
+                                         ctypes.byref(b), 16, n, rows, cols, len(widths), None)
+
+    assert call(100, [300, 200]) == sg.ERR_INVALID_ARG      # widths sum to 500, not 600
+    assert call(100, [300, 300, 0]) == sg.ERR_INVALID_ARG   # empty chunk
+    assert call(0, [600]) == sg.ERR_INVALID_ARG             # no rows per band
+    assert call(62, [600]) == sg.ERR_INVALID_ARG            # 17 bands > 16
+    assert call(100, [100] * 6) == sg.ERR_INVALID_ARG       # 6 chunks > 4
+    assert call(100, [], n=600) == sg.ERR_INVALID_ARG       # no chunks
+    assert call(100, [600], m=0) == sg.OK                    # nothing to do
+
+
 def test_selftest_wait_validation():
     # limits outside 1..10^7 microseconds are refused before any device work
     assert sg.lib().sgemm_b200_selftest_wait_timeout(0, None) == sg.ERR_INVALID_ARG

@@ -68,6 +68,23 @@ def test_plain_host_equals_device(m, n, k):
         assert sg.host_plan(m, n, k)[0] < m
 
 
+@pytest.mark.parametrize("plan", [(640, [1000, 1500, 500]), (3001, [3000]), (200, [128, 2872]),
+                                  (1024, [512, 512, 512, 1464])])
+def test_host_planned_equals_device(plan):
+    # every valid block plan gives the device entry point's bits
+    m, n, k = 3001, 3000, 700
+    A, B, C = (oracle.fill(m, k, 12, 1, 0), oracle.fill(k, n, 12, 2, 0),
+               oracle.fill(m, n, 12, 3, 0))
+    want = _device_result("plain", A, B, C, 1.5, 0.5)
+    torch = _torch()
+    _, hA = _host(A)
+    _, hB = _host(B)
+    _, hC = _host(C)
+    sg.sgemm_host(hA, hB, hC, 1.5, 0.5, plan=plan)
+    torch.cuda.synchronize()
+    assert np.array_equal(hC.numpy(), want)
+
+
 def test_plain_host_strided_and_canaries():
     m, n, k = 2500, 1100, 900
     A, B, C = (oracle.fill(m, k, 5, 1, 0), oracle.fill(k, n, 5, 2, 0), oracle.fill(m, n, 5, 3, 0))
