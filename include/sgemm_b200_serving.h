@@ -81,6 +81,9 @@ typedef struct {
 } sgemm_b200_server_trace_record;
 
 int sgemm_b200_server_create(sgemm_b200_server** server, const sgemm_b200_server_config* cfg);
+/* Stop the server: requests that have not reached the GPU are cancelled (they
+ * count as failed), batches in flight complete, then every resource is
+ * released.  Waits for the server's own streams only. */
 void sgemm_b200_server_destroy(sgemm_b200_server* server);
 
 /* Submit one request.  The operands are allocated from the pool at admission

@@ -330,6 +330,30 @@ static void admit(Server* s) {
     }
 }
 
+// Shutdown: requests that have not reached the GPU fail instead of waiting,
+// so that destroy ends once the batches in flight complete (called with the
+// lock held).  Admitted requests' operand fills may still be running on the
+// ingest stream; destroy synchronises it before freeing the pool.
+static void cancel_pending(Server* s) {
+    auto cancel = [&](Request* r) {
+        if (r->ready) {
+            cudaEventDestroy(r->ready);
+            r->ready = nullptr;
+        }
+        if (r->off >= 0 && r->auto_release) {
+            pool_free(&s->pool, r->off);
+            r->off = -1;
+        }
+        r->state = kFailed;
+        ++s->failed;
+        --s->outstanding;
+    };
+    for (Request* r : s->arrivals) cancel(r);
+    for (Request* r : s->ready) cancel(r);
+    s->arrivals.clear();
+    s->ready.clear();
+}
+
 static int launch_batch(Server* s, int si) {
     Slot& sl = s->slots[si];
     if (s->cfg.inject_batch_delay_ms > 0)
@@ -364,6 +388,7 @@ static void worker_loop(Server* s) {
             s->finished_slots.pop_front();
             finish_slot(s, si);
         }
+        if (s->stop) cancel_pending(s);
         admit(s);
         s->peak_waiting = std::max<int64_t>(s->peak_waiting, (int64_t)s->arrivals.size());
         int free_slot = -1;

@@ -139,3 +139,23 @@ def test_trace_accounts_for_every_request(path):
     assert pct(lat, 0.99) == pytest.approx(st["p99_ms"], abs=1e-6)
     assert pct(que, 0.99) == pytest.approx(st["queue_p99_ms"], abs=1e-6)
     assert pct(svc, 0.50) == pytest.approx(st["service_p50_ms"], abs=1e-6)
+
+
+def test_destroy_cancels_requests_that_can_never_be_admitted():
+    # two kept 4096^2 results fill the budget, so the third request waits for
+    # memory that never frees; destroy must cancel it rather than wait
+    import threading
+    import time
+    budget = 420 << 20
+    srv = sg.Server(budget, slots=2, max_batch=4, path="plain", keep_results=True)
+    for i in range(3):
+        srv.submit(4096, 4096, 4096, seed=i)
+    t_end = time.time() + 30
+    while srv.stats()["completed"] < 2 and time.time() < t_end:
+        time.sleep(0.01)
+    st = srv.stats()
+    assert st["completed"] == 2 and st["peak_waiting"] >= 1
+    closer = threading.Thread(target=srv.close)
+    closer.start()
+    closer.join(timeout=60)
+    assert not closer.is_alive(), "destroy waited for a request that could never run"
