@@ -727,8 +727,7 @@ int arena_launch(Arena* a, const sgemm_b200_problem* probs, int count, cudaStrea
     p.status = device_status_ptr();
     p.n_items = (int)sc.items.size();
     if (!p.status) return SGEMM_B200_ERR_CUDA;
-    static int per_sm = 0;
-    if (!per_sm) per_sm = resident_per_sm(3);
+    static const int per_sm = resident_per_sm(3);  // after the attributes; once, thread-safe
     const int grid = std::max(1, std::min(device_info().sm_count * per_sm, p.n_items));
     grouped_kernel<3><<<grid, THREADS, smem_bytes<3>(), stream>>>(p);
     return cuda_status(cudaGetLastError());
