@@ -530,7 +530,21 @@ def _grouped_leg(torch, sg, sms, sm_mhz, hbm_gbs, count=512):
     }
 
 
-def _serving_leg(sg, rates, n_requests):
+def _serving_bounds(sg, path, rate, n_requests, seed, simt_gflops, tc_useful_gflops, hbm_gbs):
+    """Offered load and roofline throughput (GFLOP/s) of one serving run's
+    request mix: each request bounded by the path's compute peak (FP32 SIMT,
+    or the BF16 tensor peak / 6 for BF16x6) or by HBM for its operand bytes."""
+    shapes, gaps = sg.serving_workload(n_requests, rate, seed)
+    flops = [2.0 * m * n * k for m, n, k in shapes]
+    peak = simt_gflops if path == "plain" else tc_useful_gflops
+    roof_s = sum(max(f / (peak * 1e9), 4.0 * (m * k + k * n + m * n) / (hbm_gbs * 1e9))
+                 for f, (m, n, k) in zip(flops, shapes))
+    # offered load over the arrival span (the first gap precedes the first
+    # submission, where the server's throughput window starts)
+    return sum(flops) / sum(gaps[1:]) * 1e-9, sum(flops) / roof_s * 1e-9
+
+
+def _serving_leg(sg, rates, n_requests, simt_gflops, tc_useful_gflops, hbm_gbs):
     out = {"workload": "Poisson arrivals; 60% M~U[16,256] N=K=4096, 40% M=N=K log-uniform "
                        "[512,4096]; operands generated and resident on the device; 64 GB "
                        "budget; 2 slots, max batch 32; each server first serves 32 untimed "
@@ -542,6 +556,8 @@ def _serving_leg(sg, rates, n_requests):
             srv.run_poisson(rate, 32, seed=7)  # warm-up; the next run starts fresh stats
             st = srv.run_poisson(rate, n_requests, seed=11)
             srv.close()
+            offered, roof = _serving_bounds(sg, path, rate, n_requests, 11, simt_gflops,
+                                            tc_useful_gflops, hbm_gbs)
             out["runs"].append({
                 "path": path, "rate_per_s": rate, "requests": n_requests,
                 "completed": st["completed"], "p50_ms": round(st["p50_ms"], 3),
@@ -550,7 +566,11 @@ def _serving_leg(sg, rates, n_requests):
                 "service_p99_ms": round(st["service_p99_ms"], 3),
                 "gflops": round(st["gflops"], 1),
                 "batches": st["batches"], "max_batch": st["max_batch_size"],
-                "max_batches_in_flight": st["max_batches_in_flight"]})
+                "max_batches_in_flight": st["max_batches_in_flight"],
+                "offered_gflops": round(offered, 1), "roofline_gflops": round(roof, 1),
+                "frac_of_bound": round(st["gflops"] / min(offered, roof), 4)})
+    out["bound_note"] = ("frac_of_bound = achieved GFLOP/s / min(offered load, roofline of the "
+                         "mix); below saturation the offered load is the bound")
     return out
 
 
@@ -702,7 +722,9 @@ def run(args):
                                          args.grouped_problems)
         torch.cuda.empty_cache()
     if rank == 0 and world == 1 and not args.skip_serving:
-        result["serving"] = _serving_leg(sg, [500.0, 1000.0, 2000.0, 4000.0], 300)
+        result["serving"] = _serving_leg(sg, [500.0, 1000.0, 2000.0, 4000.0], 300,
+                                         sms * 256 * sm_max * 1e-3,
+                                         peaks["bf16_tflops"] * 1e3 / 6, peaks["hbm_gbs"])
     if rank == 0:
         print(json.dumps(result))
     if dist is not None:
