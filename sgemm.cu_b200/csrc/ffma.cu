@@ -147,15 +147,43 @@ int plain_select(int m, int n, int k, const float* A, int lda, const float* B, i
 namespace ffma {
 
 // Row copy into a 16-byte-aligned pitch (the pack step for strides TMA cannot
-// describe): block rows walk the matrix rows, threads walk the columns, so
-// every warp reads and writes contiguous runs (HBM-bound, no division).
-__global__ void pack_rows_kernel(const float* __restrict__ src, int rows, int cols, int ld_src,
-                                 float* __restrict__ dst, int ld_dst) {
-    for (int r = blockIdx.y; r < rows; r += gridDim.y) {
-        const float* s = src + (int64_t)r * ld_src;
-        float* d = dst + (int64_t)r * ld_dst;
-        for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < cols; c += gridDim.x * blockDim.x)
-            d[c] = s[c];
+// describe), for up to two matrices in one launch: block b copies rows b,
+// b + gridDim.x, ... of A's rows followed by B's; within a row the threads
+// take consecutive columns (coalesced), eight loads in flight per thread
+// before their stores.  HBM-bound; the padding columns are not written (the
+// TMA kernel reads only the first `cols` of each row).
+struct PackJob {
+    const float* src;
+    float* dst;
+    int rows, cols, ld_src, ld_dst;
+};
+
+constexpr int kPackThreads = 256;
+constexpr int kPackUnroll = 8;
+
+__global__ void __launch_bounds__(kPackThreads) pack_rows_kernel(const PackJob a, const PackJob b) {
+    const int total = a.rows + b.rows;
+    for (int r = blockIdx.x; r < total; r += gridDim.x) {
+        const bool in_a = r < a.rows;
+        const int row = in_a ? r : r - a.rows;
+        const int cols = in_a ? a.cols : b.cols;
+        const float* __restrict__ src =
+            (in_a ? a.src : b.src) + (int64_t)row * (in_a ? a.ld_src : b.ld_src);
+        float* __restrict__ dst =
+            (in_a ? a.dst : b.dst) + (int64_t)row * (in_a ? a.ld_dst : b.ld_dst);
+        for (int c0 = 0; c0 < cols; c0 += kPackUnroll * kPackThreads) {
+            float v[kPackUnroll];
+#pragma unroll
+            for (int u = 0; u < kPackUnroll; ++u) {
+                const int c = c0 + u * kPackThreads + (int)threadIdx.x;
+                v[u] = c < cols ? src[c] : 0.0f;
+            }
+#pragma unroll
+            for (int u = 0; u < kPackUnroll; ++u) {
+                const int c = c0 + u * kPackThreads + (int)threadIdx.x;
+                if (c < cols) dst[c] = v[u];
+            }
+        }
     }
 }
 
@@ -163,11 +191,13 @@ __global__ void pack_rows_kernel(const float* __restrict__ src, int rows, int co
 // running the TMA kernel beats the 4-byte cp.async loader.
 constexpr double kPackMinWork = 134217728.0;  // 512^3
 
-static void pack(const float* src, int rows, int cols, int ld_src, float* dst, int ld_dst,
-                 cudaStream_t s) {
-    const dim3 block(256);
-    const dim3 grid(std::min(div_up(cols, 256), 16), std::min(rows, 65535));
-    pack_rows_kernel<<<grid, block, 0, s>>>(src, rows, cols, ld_src, dst, ld_dst);
+// One launch for both operands (a job with rows == 0 is skipped): eight
+// blocks per SM, each looping over rows.
+static void pack(const PackJob& a, const PackJob& b, cudaStream_t s) {
+    const int total = a.rows + b.rows;
+    const int sms = device_info().sm_count > 0 ? device_info().sm_count : 148;
+    const int grid = std::max(1, std::min(total, sms * 8));
+    pack_rows_kernel<<<grid, kPackThreads, 0, s>>>(a, b);
 }
 
 }  // namespace ffma
@@ -192,8 +222,9 @@ int plain_launch(int cfg, int m, int n, int k, float alpha, const float* A, int 
             if (e == cudaSuccess && pb)
                 e = cudaMallocFromPoolAsync(&B2, sizeof(float) * (size_t)k * ldb2, pool, stream);
             if (e == cudaSuccess) {
-                if (pa) pack(A, m, k, lda, A2, lda2, stream);
-                if (pb) pack(B, k, n, ldb, B2, ldb2, stream);
+                const PackJob ja = pa ? PackJob{A, A2, m, k, lda, lda2} : PackJob{};
+                const PackJob jb = pb ? PackJob{B, B2, k, n, ldb, ldb2} : PackJob{};
+                pack(ja, jb, stream);
                 const int s = plain_launch(-1, m, n, k, alpha, pa ? A2 : A, lda2, pb ? B2 : B,
                                            ldb2, beta, C, ldc, stream);
                 if (A2) cudaFreeAsync(A2, stream);

@@ -106,6 +106,19 @@ def test_general_strides_and_canaries(lds):
     _assert_equal(got, oracle.sgemm_basic(A, B, C, 1.5, 0.5, basic=False))
 
 
+@pytest.mark.parametrize("m,n,k,pads", [(1001, 3001, 777, (1, 1, 1)), (1003, 1500, 1201, (2, 0, 3)),
+                                        (997, 1501, 1000, (0, 1, 0))],
+                         ids=["pack_a_and_b", "pack_a", "pack_b"])
+def test_pack_path_matches_the_oracle(m, n, k, pads):
+    # row strides that are not multiples of 4 floats on problems above 512^3:
+    # the offending operands are packed to aligned rows, then the TMA kernel
+    # runs; the result is the oracle's, bit for bit
+    A, B, C = _inputs(m, n, k, 23, 0)
+    lds = (k + pads[0], n + pads[1], n + pads[2])
+    got = _run_ours(A, B, C, 1.5, 0.5, lds=lds)
+    _assert_equal(got, oracle.sgemm_basic(A, B, C, 1.5, 0.5, basic=False))
+
+
 def test_beta_zero_never_reads_c():
     m, n, k = 140, 260, 40
     A, B, _ = _inputs(m, n, k, 4, 0)
