@@ -78,7 +78,7 @@ def test_plain_bit_exact_vs_oracle(shape, ab):
     _assert_equal(got, want)
 
 
-@pytest.mark.parametrize("cfg", range(14))
+@pytest.mark.parametrize("cfg", range(len(sg.config_names())))
 @pytest.mark.parametrize("shape", [(130, 270, 77), (64, 128, 32), (300, 64, 100)],
                          ids=lambda s: "x".join(map(str, s)))
 def test_every_config_bit_exact(cfg, shape):
