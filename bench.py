@@ -595,6 +595,9 @@ def run(args):
     flush = torch.empty(int(peaks.get("l2_bytes", 256 << 20)) // 4, device="cuda")
     cfg = sg.select_config(SIZE, SIZE, SIZE, A, SIZE, B, SIZE)
     cfg_name = sg.config_names()[cfg]
+    packed = sg.packs(SIZE, SIZE, SIZE, A, SIZE, B, SIZE)  # pack step: one more launch
+    in_mb = 3 * SIZE * SIZE * 4 / 2 ** 20
+    l2_mb = peaks.get("l2_bytes", 126 << 20) / 2 ** 20
 
     # parity sample: C after one GEMM from C0 (checked by the cpu_baseline leg)
     C0_host = C0.cpu().numpy()
@@ -636,7 +639,7 @@ def run(args):
         "peak_source": f"computed: {sms} SMs x 128 FP32 lanes x 2 FLOP x SM clock "
                        f"(max {sm_max:.0f} MHz, observed median {sm_obs:.0f} MHz)",
         "kernel": cfg_name,
-        "traffic": _traffic(cfg_name),
+        "traffic": _traffic(f"{cfg_name}@{SIZE}"),
         "algorithmic_bytes": 4 * 4 * SIZE * SIZE,
     }
 
@@ -648,13 +651,15 @@ def run(args):
         "config": {"workload": f"sgemm_plain_{SIZE}", "m": SIZE, "n": SIZE, "k": SIZE,
                    "alpha": ALPHA, "beta": BETA, "dist": "uniform[-1,1) seed 0",
                    "layout": "row-major NN", "kernel_config": cfg_name,
-                   "l2": "inputs 768 MB > 126 MB L2, plus an L2-sized flush between steps",
+                   "packed_operands": [x for b, x in ((1, "A"), (2, "B")) if packed & b],
+                   "l2": f"inputs {in_mb:.0f} MB {'>' if in_mb > l2_mb else '<'} "
+                         f"{l2_mb:.0f} MB L2, plus an L2-sized flush between steps",
                    "parallelism": f"replicas x{world}"},
         "p50_ms": round(statistics.median(ms), 4),
         "p99_ms": round(sorted(ms)[min(len(ms) - 1, int(0.99 * len(ms)))], 4),
         "roofline": roofline,
         "clocks": clk,
-        "gpu_launches": args.steps,
+        "gpu_launches": args.steps * (2 if packed else 1),
         "peaks_source": peak_src,
     }
 

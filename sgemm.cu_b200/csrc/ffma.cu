@@ -117,9 +117,8 @@ static double partial_wave_cost(int r, int occ) {
     return (double(r) / occ) / e;
 }
 
-int plain_select(int m, int n, int k, const float* A, int lda, const float* B, int ldb) {
+static int select_for_loader(int m, int n, int k, int loader) {
     using namespace ffma;
-    const int loader = (k == 0 || tma_ok(A, lda, B, ldb)) ? kLoaderTma : kLoaderAsync4;
     const DeviceInfo& d = device_info();
     const int sms = d.sm_count > 0 ? d.sm_count : 148;
     int best = -1;
@@ -142,6 +141,12 @@ int plain_select(int m, int n, int k, const float* A, int lda, const float* B, i
     }
     (void)k;
     return best;
+}
+
+int plain_select(int m, int n, int k, const float* A, int lda, const float* B, int ldb) {
+    using namespace ffma;
+    const int loader = (k == 0 || tma_ok(A, lda, B, ldb)) ? kLoaderTma : kLoaderAsync4;
+    return select_for_loader(m, n, k, loader);
 }
 
 namespace ffma {
@@ -191,6 +196,15 @@ __global__ void __launch_bounds__(kPackThreads) pack_rows_kernel(const PackJob a
 // running the TMA kernel beats the 4-byte cp.async loader.
 constexpr double kPackMinWork = 134217728.0;  // 512^3
 
+// Operands the plain path copies to aligned rows before its TMA kernel:
+// bit 0 A, bit 1 B; 0 when the kernel reads them in place.
+static int pack_mask(int m, int n, int k, const float* A, int lda, const float* B, int ldb) {
+    if (k <= 0 || tma_ok(A, lda, B, ldb) || double(m) * n * k < kPackMinWork) return 0;
+    const bool pa = (lda % 4 != 0) || (reinterpret_cast<uintptr_t>(A) % 16 != 0);
+    const bool pb = (ldb % 4 != 0) || (reinterpret_cast<uintptr_t>(B) % 16 != 0);
+    return (pa ? 1 : 0) | (pb ? 2 : 0);
+}
+
 // One launch for both operands (a job with rows == 0 is skipped): eight
 // blocks per SM, each looping over rows.
 static void pack(const PackJob& a, const PackJob& b, cudaStream_t s) {
@@ -207,14 +221,14 @@ int plain_launch(int cfg, int m, int n, int k, float alpha, const float* A, int 
     using namespace ffma;
     if (m == 0 || n == 0) return SGEMM_B200_OK;
     if (!device_is_sm100()) return SGEMM_B200_ERR_UNSUPPORTED;
-    if (cfg < 0 && k > 0 && !tma_ok(A, lda, B, ldb) && double(m) * n * k >= kPackMinWork) {
+    const int mask = cfg < 0 ? pack_mask(m, n, k, A, lda, B, ldb) : 0;
+    if (mask) {
         // Unaligned strides on a large problem: copy the offending operand(s) to
         // 16-byte-aligned rows (stream-ordered scratch from the library pool)
         // and run the TMA kernel.  Same arithmetic, same bits.
         cudaMemPool_t pool = library_pool();
         if (pool) {
-            const bool pa = (lda % 4 != 0) || (reinterpret_cast<uintptr_t>(A) % 16 != 0);
-            const bool pb = (ldb % 4 != 0) || (reinterpret_cast<uintptr_t>(B) % 16 != 0);
+            const bool pa = (mask & 1) != 0, pb = (mask & 2) != 0;
             const int lda2 = pa ? (k + 3) / 4 * 4 : lda, ldb2 = pb ? (n + 3) / 4 * 4 : ldb;
             float *A2 = nullptr, *B2 = nullptr;
             cudaError_t e = cudaSuccess;
@@ -314,5 +328,14 @@ extern "C" int sgemm_b200_select_config(int m, int n, int k, const float* A, int
     (void)C;
     (void)ldc;
     if (m <= 0 || n <= 0 || k < 0) return -1;
+    // the kernel that runs: after a pack step the operands are TMA-aligned
+    if (sgb::ffma::pack_mask(m, n, k, A, lda, B, ldb))
+        return sgb::select_for_loader(m, n, k, sgb::ffma::kLoaderTma);
     return sgb::plain_select(m, n, k, A, lda, B, ldb);
+}
+
+extern "C" int sgemm_b200_packs(int m, int n, int k, const float* A, int lda, const float* B,
+                                int ldb) {
+    if (m <= 0 || n <= 0 || k < 0) return 0;
+    return sgb::ffma::pack_mask(m, n, k, A, lda, B, ldb);
 }

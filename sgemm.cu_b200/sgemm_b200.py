@@ -114,6 +114,7 @@ def _declare(lib: ctypes.CDLL) -> None:
     d("sgemm_b200_config_count", _I, [])
     d("sgemm_b200_config_name", ctypes.c_char_p, [_I])
     d("sgemm_b200_select_config", _I, [_I, _I, _I, _P, _I, _P, _I, _P, _I])
+    d("sgemm_b200_packs", _I, [_I, _I, _I, _P, _I, _P, _I])
     d("sgemm_b200_basic", _I, _GEMM_ARGS + [_P])
     d("sgemm_b200_split_workspace_size", ctypes.c_size_t, [_I, _I, _I, _I])
     d("sgemm_b200_split", _I, [_I] + _GEMM_ARGS + [_P, ctypes.c_size_t, _P])
@@ -319,9 +320,17 @@ def config_names() -> list:
 
 
 def select_config(m: int, n: int, k: int, A=None, lda: int = 0, B=None, ldb: int = 0) -> int:
+    """Config id of the kernel sgemm() runs (after a pack step, if any)."""
     pa = A.data_ptr() if A is not None else 16
     pb = B.data_ptr() if B is not None else 16
     return lib().sgemm_b200_select_config(m, n, k, pa, lda or k, pb, ldb or n, None, n)
+
+
+def packs(m: int, n: int, k: int, A=None, lda: int = 0, B=None, ldb: int = 0) -> int:
+    """Operands sgemm() copies to aligned rows first: bit 0 A, bit 1 B."""
+    pa = A.data_ptr() if A is not None else 16
+    pb = B.data_ptr() if B is not None else 16
+    return lib().sgemm_b200_packs(m, n, k, pa, lda or k, pb, ldb or n)
 
 
 def selftest_wait_timeout(limit_us: int, stream=None) -> None:
