@@ -397,14 +397,27 @@ static void worker_loop(Server* s) {
                 free_slot = (int)i;
                 break;
             }
+        // With a batch already on the GPU, a new batch takes only requests whose
+        // operands are in place: one whose generation is still running would
+        // hold the slot, and the GPU, behind it.  Generation runs in admission
+        // order on one stream, so those requests are a prefix of the queue.
+        // With the GPU idle, a batch takes what is queued and its launch waits
+        // on the device.
+        bool wait_for_operands = false;
         if (free_slot >= 0 && !s->ready.empty()) {
             Slot& sl = s->slots[free_slot];
+            const bool gpu_idle = s->in_flight == 0;
             while (!s->ready.empty() && (int)sl.batch.size() < s->cfg.max_batch) {
                 Request* r = s->ready.front();
+                if (!gpu_idle && cudaEventQuery(r->ready) == cudaErrorNotReady) break;
                 s->ready.pop_front();
                 r->state = kRunning;
                 sl.batch.push_back(r);
             }
+            wait_for_operands = sl.batch.empty();
+        }
+        if (free_slot >= 0 && !s->slots[free_slot].batch.empty()) {
+            Slot& sl = s->slots[free_slot];
             sl.busy = true;
             ++s->in_flight;
             ++s->batches;
@@ -449,7 +462,10 @@ static void worker_loop(Server* s) {
         }
         if (s->outstanding == 0) s->cv_drain.notify_all();
         if (s->stop && s->outstanding == 0) break;
-        s->cv.wait_for(lock, std::chrono::milliseconds(2));
+        if (wait_for_operands)
+            s->cv.wait_for(lock, std::chrono::microseconds(20));
+        else
+            s->cv.wait_for(lock, std::chrono::milliseconds(2));
     }
 }
 
