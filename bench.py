@@ -310,6 +310,20 @@ def _cpu_baseline_and_checks(torch, sg, C_after, C0_host, size, checks, target_s
     sub = rows[np.linspace(0, nrows - 1, min(256, nrows)).astype(np.int64)]
     ref, mag = oracle.dgemm(hA, hB, C0_host[sub], ALPHA, BETA, row_ids=sub)
     err = oracle.error_stats(C_after[sub], ref, mag)
+    # the whole GEMM at the smaller sweep sizes on the same threads (best of 3,
+    # one run at 4096^3)
+    by_size = {}
+    for n_s in (1024, 2048, 4096):
+        if n_s >= size:
+            break
+        X = [oracle.fill(n_s, n_s, SEED, tag, 0) for tag in (1, 2, 3)]
+        best = 1e30
+        for _ in range(3 if n_s < 4096 else 1):
+            t0 = time.perf_counter()
+            oracle.sgemm_basic(X[0], X[1], X[2], ALPHA, BETA, basic=False)
+            best = min(best, time.perf_counter() - t0)
+        by_size[str(n_s)] = round(2.0 * n_s ** 3 / best * 1e-9, 2)
+        del X
     errors = {}
     for chk in checks:
         label, n_size, dist, ids, outs = chk[:5]
@@ -332,6 +346,7 @@ def _cpu_baseline_and_checks(torch, sg, C_after, C0_host, size, checks, target_s
         "sample": f"{nrows} of {size} rows of the {size}^3 GEMM (C restatement of the "
                   f"reference's kernel_basic: fmaf chain per element, OpenMP over rows)",
         "seconds": round(dt, 2),
+        "gflops_by_size": by_size,
         "parity": {"rows_checked": nrows, "elements": int(got.size), "bit_exact": exact},
         "plain_error_vs_fp64": {"rows": int(len(sub)), **{k: float(v) for k, v in err.items()}},
     }, errors
