@@ -162,7 +162,7 @@ def test_grouped_skinny_split_k_deterministic_and_accurate(tmp_path):
 
 
 def _workload(n, seed):
-    """M, N, K log-uniform on [64, 4096], multiples of 8."""
+    """The 512-problem grouped workload: M, N, K log-uniform on [64, 4096], multiples of 8."""
     rng = np.random.default_rng(seed)
     vals = np.exp(rng.uniform(np.log(64), np.log(4096), size=(n, 3)))
     return [tuple(int(max(8, round(v / 8) * 8)) for v in row) for row in vals]

@@ -1,7 +1,7 @@
 """GPU tests of the split-precision tensor-core paths (BF16x6, TF32x3).
 
 No reference counterpart exists (the reference has no tensor-core path); the
-contract is sgemm()'s (src/sgemm.cuh:19-30).  Accuracy is judged against the
+contract is sgemm()'s (src/sgemm.cuh:19-30).  Accuracy is measured against the
 FP64 oracle with the componentwise metric
     max |c - c64| / (|alpha| (|A||B|)_ij + |beta| |C0|_ij)
 next to the plain FFMA path's error on the same inputs.
