@@ -422,7 +422,7 @@ def _config_1024_leg(torch, sg, steps, warmup):
         sg.sgemm_host(hA, hB, hC, 1.0, 0.0)
 
     te = _time_steps(torch, host_step, steps, warmup, flush)
-    cfg = sg.config_names()[sg.select_config(n, n, n, A, n, B, n)]
+    cfg = sg.config_names()[sg.select_config(n, n, n, A, n, B, n, beta=0.0)]
     res = {"gflops": round(2.0 * n ** 3 / (t * 1e-3) * 1e-9, 1), "ms_per_step": round(t, 4),
            "e2e_gflops": round(2.0 * n ** 3 / (statistics.mean(te) * 1e-3) * 1e-9, 1),
            "kernel_config": cfg, "alpha": 1.0, "beta": 0.0,
@@ -608,7 +608,7 @@ def run(args):
     A, B, C = _alloc_inputs(torch, sg, SIZE)
     C0 = C.clone()
     flush = torch.empty(int(peaks.get("l2_bytes", 256 << 20)) // 4, device="cuda")
-    cfg = sg.select_config(SIZE, SIZE, SIZE, A, SIZE, B, SIZE)
+    cfg = sg.select_config(SIZE, SIZE, SIZE, A, SIZE, B, SIZE, beta=BETA)
     cfg_name = sg.config_names()[cfg]
     packed = sg.packs(SIZE, SIZE, SIZE, A, SIZE, B, SIZE)  # pack step: one more launch
     in_mb = 3 * SIZE * SIZE * 4 / 2 ** 20

@@ -86,15 +86,17 @@ int sgemm_b200_with_config(int cfg, int m, int n, int k,
  * (e.g. "tma_128x64_w4_t8x8_s3"). */
 int sgemm_b200_config_count(void);
 const char* sgemm_b200_config_name(int cfg);
-/* Configuration of the kernel sgemm_b200 runs for this shape and these
- * pointers (host-only).  Strides that TMA cannot describe (not a multiple of
- * 4 floats, or a base not 16-byte aligned) on problems of at least 512^3 are
- * first copied to aligned rows (see sgemm_b200_packs), so the answer is then
- * a TMA configuration; smaller such problems use a cp.async configuration. */
+/* Configuration of the kernel sgemm_b200 runs for this shape, these
+ * pointers and this beta (host-only; beta is a host pointer as in
+ * sgemm_b200, NULL meaning C is read).  Strides that TMA cannot describe (not
+ * a multiple of 4 floats, or a base not 16-byte aligned) on problems of at
+ * least 512^3 are first copied to aligned rows (see sgemm_b200_packs), so the
+ * answer is then a TMA configuration; smaller such problems use a cp.async
+ * configuration. */
 int sgemm_b200_select_config(int m, int n, int k,
                              const float* A, int lda,
                              const float* B, int ldb,
-                             const float* C, int ldc);
+                             const float* beta);
 
 /* Operands sgemm_b200 copies to aligned rows before its kernel (host-only):
  * bit 0 for A, bit 1 for B, 0 when both are read in place.  The copy is one

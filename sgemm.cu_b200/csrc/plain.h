@@ -9,7 +9,8 @@ namespace sgb {
 int plain_config_count();
 const char* plain_config_name(int cfg);
 int plain_config_tile(int cfg, int* bm, int* bn);
-int plain_select(int m, int n, int k, const float* A, int lda, const float* B, int ldb);
+int plain_select(int m, int n, int k, const float* A, int lda, const float* B, int ldb,
+                 bool reads_c);
 int plain_launch(int cfg, int m, int n, int k, float alpha, const float* A, int lda,
                  const float* B, int ldb, float beta, float* C, int ldc, cudaStream_t stream);
 

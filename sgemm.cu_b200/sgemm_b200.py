@@ -113,7 +113,7 @@ def _declare(lib: ctypes.CDLL) -> None:
     d("sgemm_b200_with_config", _I, [_I] + _GEMM_ARGS + [_P])
     d("sgemm_b200_config_count", _I, [])
     d("sgemm_b200_config_name", ctypes.c_char_p, [_I])
-    d("sgemm_b200_select_config", _I, [_I, _I, _I, _P, _I, _P, _I, _P, _I])
+    d("sgemm_b200_select_config", _I, [_I, _I, _I, _P, _I, _P, _I, _FP])
     d("sgemm_b200_packs", _I, [_I, _I, _I, _P, _I, _P, _I])
     d("sgemm_b200_basic", _I, _GEMM_ARGS + [_P])
     d("sgemm_b200_split_workspace_size", ctypes.c_size_t, [_I, _I, _I, _I])
@@ -319,11 +319,14 @@ def config_names() -> list:
     return [l.sgemm_b200_config_name(i).decode() for i in range(l.sgemm_b200_config_count())]
 
 
-def select_config(m: int, n: int, k: int, A=None, lda: int = 0, B=None, ldb: int = 0) -> int:
-    """Config id of the kernel sgemm() runs (after a pack step, if any)."""
+def select_config(m: int, n: int, k: int, A=None, lda: int = 0, B=None, ldb: int = 0,
+                  beta: Optional[float] = None) -> int:
+    """Config id of the kernel sgemm() runs (after a pack step, if any) for
+    this beta (None: C is read)."""
     pa = A.data_ptr() if A is not None else 16
     pb = B.data_ptr() if B is not None else 16
-    return lib().sgemm_b200_select_config(m, n, k, pa, lda or k, pb, ldb or n, None, n)
+    return lib().sgemm_b200_select_config(m, n, k, pa, lda or k, pb, ldb or n,
+                                          None if beta is None else _f(beta))
 
 
 def packs(m: int, n: int, k: int, A=None, lda: int = 0, B=None, ldb: int = 0) -> int:

@@ -87,16 +87,16 @@ def test_config_table():
     l = sg.lib()
     # unaligned strides: small problems run a cp.async configuration in place;
     # from 512^3 the offending operands are packed and a TMA configuration runs
-    c = l.sgemm_b200_select_config(300, 301, 299, 16, 299, 16, 301, 16, 301)
+    c = l.sgemm_b200_select_config(300, 301, 299, 16, 299, 16, 301, None)
     assert names[c].startswith("cpa_") and l.sgemm_b200_packs(300, 301, 299, 16, 299, 16, 301) == 0
-    c = l.sgemm_b200_select_config(3001, 3001, 3001, 16, 3001, 16, 3001, 16, 3001)
+    c = l.sgemm_b200_select_config(3001, 3001, 3001, 16, 3001, 16, 3001, None)
     assert names[c].startswith("tma_") and l.sgemm_b200_packs(3001, 3001, 3001, 16, 3001, 16,
                                                               3001) == 3
     assert l.sgemm_b200_packs(3001, 3000, 3001, 16, 3001, 16, 3000) == 1  # A only
     assert l.sgemm_b200_packs(3000, 3001, 3000, 16, 3000, 16, 3001) == 2  # B only
     assert l.sgemm_b200_packs(3001, 3001, 3001, 16, 3004, 16, 3004) == 0  # padded pitches
     assert l.sgemm_b200_packs(3000, 3000, 3000, 20, 3000, 16, 3000) == 1  # A base not 16-aligned
-    c = l.sgemm_b200_select_config(8192, 8192, 8192, 16, 8192, 16, 8192, 16, 8192)
+    c = l.sgemm_b200_select_config(8192, 8192, 8192, 16, 8192, 16, 8192, None)
     assert names[c].startswith("tma_") and l.sgemm_b200_packs(8192, 8192, 8192, 16, 8192, 16,
                                                               8192) == 0
 
