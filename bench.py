@@ -165,6 +165,18 @@ def _traffic(kernel_key: str):
         return None
 
 
+def _config(world: int, kernel_config: str, l2_bytes: float) -> dict:
+    """The workload's config, identical in both arms except `kernel_config`."""
+    in_mb = 3 * SIZE * SIZE * 4 / 2 ** 20
+    l2_mb = l2_bytes / 2 ** 20
+    return {"workload": f"sgemm_plain_{SIZE}", "m": SIZE, "n": SIZE, "k": SIZE,
+            "alpha": ALPHA, "beta": BETA, "dist": "uniform[-1,1) seed 0",
+            "layout": "row-major NN", "kernel_config": kernel_config,
+            "l2": f"inputs {in_mb:.0f} MB {'>' if in_mb > l2_mb else '<'} "
+                  f"{l2_mb:.0f} MB L2, plus an L2-sized flush between steps",
+            "parallelism": f"replicas x{world}"}
+
+
 # -------------------------------------------------------------- device legs --
 
 def _alloc_inputs(torch, sg, size):
@@ -352,6 +364,43 @@ def _cpu_baseline_and_checks(torch, sg, C_after, C0_host, size, checks, target_s
     }, errors
 
 
+def _library_leg(torch, A, B, C0, flush, steps):
+    """Library context numbers on the same 8192^3 problem (not this library's
+    kernels): cuBLAS FP32 GEMM with the default math mode (the reference's
+    -DCUBLAS=1 lane, benchmark.cu:150-164; torch's addmm with TF32 off), and
+    the dense TF32 and BF16 tensor-core rates of a library matmul, measured
+    here to give the split paths' rooflines."""
+    out = {}
+    prev = torch.backends.cuda.matmul.allow_tf32
+    try:
+        torch.backends.cuda.matmul.allow_tf32 = False
+        C = C0.clone()
+        ms = _time_steps(torch, lambda: C.addmm_(A, B, beta=BETA, alpha=ALPHA), steps, 3, flush)
+        t = statistics.mean(ms)
+        out["cublas_sgemm"] = {"gflops": round(2.0 * SIZE ** 3 / (t * 1e-3) * 1e-9, 1),
+                               "ms_per_step": round(t, 4),
+                               "api": "torch addmm, FP32, TF32 off (cuBLAS default math)"}
+        del C
+        torch.backends.cuda.matmul.allow_tf32 = True
+        X = torch.empty_like(A)
+        ms = _time_steps(torch, lambda: torch.mm(A, B, out=X), steps, 3, flush)
+        t = statistics.mean(ms)
+        out["tf32_tflops"] = round(2.0 * SIZE ** 3 / (t * 1e-3) * 1e-12, 1)
+        Ab, Bb = A.bfloat16(), B.bfloat16()
+        Xb = torch.empty_like(Ab)
+        ms = _time_steps(torch, lambda: torch.mm(Ab, Bb, out=Xb), steps, 3, flush)
+        t = statistics.mean(ms)
+        out["bf16_tflops"] = round(2.0 * SIZE ** 3 / (t * 1e-3) * 1e-12, 1)
+        out["note"] = ("library GEMMs timed like the plain path (CUDA events per step, L2 flush "
+                       "between steps), at M=N=K=%d; tf32/bf16 are dense tensor-core rates" % SIZE)
+        del X, Ab, Bb, Xb
+    except Exception as e:  # report, never hide
+        out["error"] = str(e)
+    finally:
+        torch.backends.cuda.matmul.allow_tf32 = prev
+    return out
+
+
 def _split_leg(torch, sg, A, B, C0, flush, steps, warmup, rows, peaks, local):
     """BF16x6 / TF32x3 on the same problem: GFLOP/s against the tensor-core
     roofline, plus sampled output rows (C after one call from C0) that the
@@ -378,7 +427,9 @@ def _split_leg(torch, sg, A, B, C0, flush, steps, warmup, rows, peaks, local):
             t = statistics.mean(ms)
             gf = 2.0 * SIZE ** 3 / (t * 1e-3) * 1e-9
             prods = 6 if name == "bf16x6" else 3
-            rate = 1.0 if name == "bf16x6" else 0.5
+            # TF32: the library TF32 rate measured here over its BF16 rate,
+            # applied to the BF16 peaks (half, if it was not measured)
+            rate = 1.0 if name == "bf16x6" else peaks.get("tf32_over_bf16", 0.5)
             tc_peak = peaks["bf16_tflops"] * rate
             tc_sus = peaks.get("bf16_tflops_sustained", peaks["bf16_tflops"]) * rate
             out[name] = {"gflops": round(gf, 1), "ms_per_step": round(t, 4),
@@ -388,9 +439,11 @@ def _split_leg(torch, sg, A, B, C0, flush, steps, warmup, rows, peaks, local):
                          "useful_roofline_sustained_tflops": round(tc_sus / prods, 1),
                          "frac_of_useful_roofline_sustained":
                              round(gf * 1e-3 / (tc_sus / prods), 4),
-                         "roofline_note": "BF16 dense peak (measured, burst and sustained under "
-                                          "the power cap) / products; TF32 taken as half the "
-                                          "BF16 rate",
+                         "roofline_note": "BF16 dense peak (burst and sustained under the "
+                                          "power cap) / products; for TF32 that peak times the "
+                                          "library TF32/BF16 rate ratio measured in this run "
+                                          "(library leg)",
+                         "tf32_over_bf16": peaks.get("tf32_over_bf16"),
                          "clocks": clk,
                          "error_vs_fp64_sampled_rows": None}
             del ws
@@ -611,8 +664,6 @@ def run(args):
     cfg = sg.select_config(SIZE, SIZE, SIZE, A, SIZE, B, SIZE, beta=BETA)
     cfg_name = sg.config_names()[cfg]
     packed = sg.packs(SIZE, SIZE, SIZE, A, SIZE, B, SIZE)  # pack step: one more launch
-    in_mb = 3 * SIZE * SIZE * 4 / 2 ** 20
-    l2_mb = peaks.get("l2_bytes", 126 << 20) / 2 ** 20
 
     # parity sample: C after one GEMM from C0 (checked by the cpu_baseline leg)
     C0_host = C0.cpu().numpy()
@@ -663,13 +714,8 @@ def run(args):
         "value": round(value, 1), "unit": "GFLOP/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms_step, 4), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": f"sgemm_plain_{SIZE}", "m": SIZE, "n": SIZE, "k": SIZE,
-                   "alpha": ALPHA, "beta": BETA, "dist": "uniform[-1,1) seed 0",
-                   "layout": "row-major NN", "kernel_config": cfg_name,
-                   "packed_operands": [x for b, x in ((1, "A"), (2, "B")) if packed & b],
-                   "l2": f"inputs {in_mb:.0f} MB {'>' if in_mb > l2_mb else '<'} "
-                         f"{l2_mb:.0f} MB L2, plus an L2-sized flush between steps",
-                   "parallelism": f"replicas x{world}"},
+        "config": _config(world, cfg_name, peaks.get("l2_bytes", 126 << 20)),
+        "packed_operands": [x for b, x in ((1, "A"), (2, "B")) if packed & b],
         "p50_ms": round(statistics.median(ms), 4),
         "p99_ms": round(sorted(ms)[min(len(ms) - 1, int(0.99 * len(ms)))], 4),
         "roofline": roofline,
@@ -702,12 +748,24 @@ def run(args):
                          "copy_then_sgemm": {
                              "value": round(flops * world / (seq_ms * 1e-3) * 1e-9, 1),
                              "ms_per_step": round(seq_ms, 3)}}
+        # the reference callers' own sequence with this library's kernel, beside
+        # the pipelined e2e: the kernel's share of the end-to-end gain
+        result["e2e_copy_then_sgemm"] = {
+            "value": round(flops * world / (seq_ms * 1e-3) * 1e-9, 1), "unit": "GFLOP/s",
+            "ms_per_step": round(seq_ms, 3), "h2d_bytes_per_step": h2d,
+            "d2h_bytes_per_step": d2h,
+            "api": "copy A, B, C in (cudaMemcpyAsync), sgemm_b200, copy C out"}
 
     checks = []
     if rank == 0 and world == 1:
         result["config_1024"], chk = _config_1024_leg(torch, sg, max(20, args.steps), args.warmup)
         checks.append(chk)
     split_rows = np.linspace(0, SIZE - 1, 64).astype(np.int32)
+    if rank == 0 and world == 1 and not args.skip_library:
+        result["library"] = _library_leg(torch, A, B, C0, flush, max(10, args.steps // 2))
+        lib = result["library"]
+        if lib.get("tf32_tflops") and lib.get("bf16_tflops"):
+            peaks = dict(peaks, tf32_over_bf16=round(lib["tf32_tflops"] / lib["bf16_tflops"], 4))
     if rank == 0 and not args.skip_split:
         result["split"], samples = _split_leg(torch, sg, A, B, C0, flush,
                                               max(20, 2 * args.steps), args.warmup, split_rows,
@@ -751,8 +809,26 @@ def run(args):
         dist.destroy_process_group()
 
 
+def _host_inputs(torch, size):
+    """A, B, C from the oracle's copy of the seeded generator (seed 0, tags
+    1, 2, 3, uniform[-1, 1)) -- the same bits the library's device fill writes
+    -- copied to the device.  The reference arm uses this so that it loads
+    nothing of this repository's library."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    out = []
+    for tag in (1, 2, 3):
+        h = torch.from_numpy(oracle.fill(size, size, SEED, tag, 0))
+        out.append(h.cuda())
+        del h
+    torch.cuda.synchronize()
+    return out
+
+
 def run_reference(args, torch, peaks, sms, local):
-    """The reference's own sgemm() built from its sources, same workload."""
+    """The reference's own sgemm() built from its sources, same workload.
+    Nothing of this repository's library is loaded in this arm: inputs come
+    from the oracle's host generator, the GEMM from oracle/_ref."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
     try:
@@ -760,9 +836,8 @@ def run_reference(args, torch, peaks, sms, local):
     except Exception as e:
         print(json.dumps({"impl": "reference", "unavailable": f"reference build missing: {e}"}))
         return
-    import sgemm_b200 as sg  # only for the seeded fill of the inputs
-    A, B, C = _alloc_inputs(torch, sg, SIZE)
-    flush = torch.empty((256 << 20) // 4, device="cuda")
+    A, B, C = _host_inputs(torch, SIZE)
+    flush = torch.empty(int(peaks.get("l2_bytes", 256 << 20)) // 4, device="cuda")
 
     def step():
         oracle.ref_sgemm(A, B, C, ALPHA, BETA)
@@ -778,30 +853,30 @@ def run_reference(args, torch, peaks, sms, local):
                             max(3, args.steps // 5), 2, SIZE)
     sm_max = clk.get("sm_max_mhz") or peaks.get("sm_max_mhz", 1965.0)
     peak = sms * 256 * sm_max * 1e-3
+    kernel = ("reference sgemm_128x256x8 (src/sgemm.cuh:41-44)"
+              if oracle.ref().ref_sgemm_kernel_choice(SIZE, SIZE) == 1
+              else "reference sgemm_128x128x8 (src/sgemm.cuh:45-47)")
     result = {
         "impl": "reference",
         "metric": f"plain FFMA SGEMM GFLOP/s at M=N=K={SIZE} (alpha=1.5, beta=0.5)",
         "value": round(value, 1), "unit": "GFLOP/s", "n_gpus": 1, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(t, 4), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": f"sgemm_plain_{SIZE}", "m": SIZE, "n": SIZE, "k": SIZE,
-                   "alpha": ALPHA, "beta": BETA, "dist": "uniform[-1,1) seed 0",
-                   "kernel_config": ("reference sgemm_128x256x8 (src/sgemm.cuh:41-44)"
-                                     if oracle.ref().ref_sgemm_kernel_choice(SIZE, SIZE) == 1
-                                     else "reference sgemm_128x128x8 (src/sgemm.cuh:45-47)"),
-                   "l2": "inputs 768 MB > 126 MB L2, plus an L2-sized flush between steps"},
+        "config": _config(1, kernel, peaks.get("l2_bytes", 126 << 20)),
         "roofline": {"bound": "fp32_simt", "unit": "TFLOP/s", "achieved": round(value * 1e-3, 2),
                      "peak": round(peak * 1e-3, 2), "frac": round(value / peak, 4),
                      "traffic": None},
         "clocks": clk,
         "e2e": {"value": round(flops / (ms_e2e * 1e-3) * 1e-9, 1), "unit": "GFLOP/s",
                 "ms_per_step": round(ms_e2e, 3), "h2d_bytes_per_step": h2d,
-                "d2h_bytes_per_step": d2h},
+                "d2h_bytes_per_step": d2h,
+                "api": "the reference callers' sequence: copy A, B, C in, sgemm(), copy C out"},
         "cpu_baseline": {"value": round(value, 1), "unit": "GFLOP/s", "cores": None,
                          "kind": "reference",
                          "sample": "the reference has no CPU GEMM (its test oracle is the GPU "
                                    "kernel_basic); this arm runs its own sgemm() kernels, built "
-                                   "from its sources for sm_100a, on the B200"},
+                                   "from its sources for sm_100a, on the B200, with inputs from "
+                                   "the oracle's host generator"},
     }
     print(json.dumps(result))
 
@@ -818,6 +893,8 @@ def main():
     ap.add_argument("--skip-split-configs", action="store_true",
                     help="skip the 8192^3 / 16384^3 signed-power-of-two split configs")
     ap.add_argument("--skip-e2e", action="store_true")
+    ap.add_argument("--skip-library", action="store_true",
+                    help="skip the cuBLAS / library tensor-core context numbers")
     ap.add_argument("--skip-grouped", action="store_true")
     ap.add_argument("--skip-serving", action="store_true")
     ap.add_argument("--grouped-problems", type=int, default=512,

@@ -29,6 +29,13 @@
 extern "C" {
 #endif
 
+/* Version of this C ABI.  It changes whenever an existing entry point changes
+ * its parameters or their meaning (new entry points keep it); a caller
+ * compiled against one header can compare it with sgemm_b200_abi_version()
+ * at run time. */
+#define SGEMM_B200_ABI_VERSION 2
+int sgemm_b200_abi_version(void);
+
 /* cudaStream_t without pulling in the CUDA headers: the ABI takes it as an
  * opaque pointer (NULL = the legacy default stream). */
 typedef void* sgemm_b200_stream_t;
@@ -86,17 +93,25 @@ int sgemm_b200_with_config(int cfg, int m, int n, int k,
  * (e.g. "tma_128x64_w4_t8x8_s3"). */
 int sgemm_b200_config_count(void);
 const char* sgemm_b200_config_name(int cfg);
-/* Configuration of the kernel sgemm_b200 runs for this shape, these
- * pointers and this beta (host-only; beta is a host pointer as in
- * sgemm_b200, NULL meaning C is read).  Strides that TMA cannot describe (not
- * a multiple of 4 floats, or a base not 16-byte aligned) on problems of at
- * least 512^3 are first copied to aligned rows (see sgemm_b200_packs), so the
- * answer is then a TMA configuration; smaller such problems use a cp.async
- * configuration. */
+/* Configuration of the kernel sgemm_b200 runs for this shape and these
+ * pointers when C is read (beta != 0); host-only.  C and ldc are not used
+ * (kept for callers of the first form of this query).  Strides that TMA
+ * cannot describe (not a multiple of 4 floats, or a base not 16-byte aligned)
+ * on problems of at least 512^3 are first copied to aligned rows (see
+ * sgemm_b200_packs), so the answer is then a TMA configuration; smaller such
+ * problems use a cp.async configuration. */
 int sgemm_b200_select_config(int m, int n, int k,
                              const float* A, int lda,
                              const float* B, int ldb,
-                             const float* beta);
+                             const float* C, int ldc);
+/* The same query for a given beta (a host pointer, as in sgemm_b200; NULL
+ * means C is read): with beta == 0 the dispatcher may pick another tile,
+ * because an epilogue that only writes C changes which tile finishes first
+ * when the problem is a single partial wave. */
+int sgemm_b200_select_config_beta(int m, int n, int k,
+                                  const float* A, int lda,
+                                  const float* B, int ldb,
+                                  const float* beta);
 
 /* Operands sgemm_b200 copies to aligned rows before its kernel (host-only):
  * bit 0 for A, bit 1 for B, 0 when both are read in place.  The copy is one
@@ -148,12 +163,15 @@ int sgemm_b200_split(int path, int m, int n, int k,
  * deployments that must not fail for lack of memory at run time.
  *
  * Same arguments and result as sgemm_b200_split, but the split operand planes
- * go to one static 64 MiB device array inside this library instead of a
- * workspace: the call makes no cudaMalloc, cudaFree or other allocation.  The
- * array exists on every GPU that loads this library until the process exits.
- * Problems whose planes need more than 64 MiB
- * (sgemm_b200_split_workspace_size(path, m, n, k) > 64 MiB, e.g. BF16X6
- * beyond about m = n = k = 2048) are refused with SGEMM_B200_ERR_NO_MEMORY.
+ * go to one static device array inside this library instead of a workspace:
+ * the call makes no cudaMalloc, cudaFree or other allocation.  The array
+ * (64 MiB of planes plus 1 KiB of base alignment) exists on every GPU that
+ * loads this library until the process exits.  A problem is accepted when
+ * sgemm_b200_split_workspace_size(path, m, n, k) <= 64 MiB + 1 KiB, i.e. its
+ * planes fit in 64 MiB: cubes up to m = n = k = 2048 for TF32X3 (planes of
+ * exactly 64 MiB) and 2361 for BF16X6; larger problems are refused with
+ * SGEMM_B200_ERR_NO_MEMORY before any work is enqueued.  k == 0 (C := beta*C)
+ * needs no planes and is always accepted.
  * The first call on each device looks up the array's device address (with
  * that device current); make that first call before any stream capture.
  * Every call shares the one array, so calls whose work overlaps on the GPU
@@ -301,6 +319,14 @@ typedef enum {
 int sgemm_b200_fill_random(float* X, int rows, int cols, int ld,
                            uint64_t seed, uint32_t tag, int dist,
                            sgemm_b200_stream_t stream);
+
+/* Bytes the library's own stream-ordered memory pool on the current device
+ * holds for live allocations (*used_bytes) and keeps reserved from the driver
+ * (*reserved_bytes).  The pool backs the scratch the library allocates itself:
+ * split workspaces when the caller passes none, packed copies of unaligned
+ * operands, and the host-operand path's staging.  Both are 0 before any call
+ * on the device has created the pool; the query never creates it. */
+int sgemm_b200_pool_usage(size_t* used_bytes, size_t* reserved_bytes);
 
 /* Reads and clears the device-side status word that bounded waits set on
  * expiry (SGEMM_B200_OK or SGEMM_B200_ERR_TIMEOUT).  Synchronises the device. */

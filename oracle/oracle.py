@@ -7,6 +7,10 @@
   _ref/libref_sgemm.so
                      the reference's own sgemm()/sgemm_basic() compiled for
                      sm_100a from its sources (ref_sgemm.cu)
+  _ref/libref_sgemm_v{1,2,3}.so
+                     the same sources with their PTX macros given a "memory"
+                     clobber (ref_sgemm_variant.cu): loads only, stores only,
+                     all -- used to locate the sgemm_128x128x8 defect
 
 Only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline leg (and its
 reference arm, which times the reference itself) may use this module, and only
@@ -28,6 +32,7 @@ REF_LIB = os.path.join(HERE, "_ref", "libref_sgemm.so")
 _cpu = None
 _gpu = None
 _ref = None
+_ref_variants = {}
 
 _F32P = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
 _F64P = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
@@ -143,8 +148,9 @@ def gpu() -> ctypes.CDLL:
     return _gpu
 
 
-def gpu_error_stats(A, B, C0, C, alpha: float, beta: float) -> dict:
-    """Full-matrix FP64 error of C (torch CUDA tensors) against alpha*A@B + beta*C0."""
+def gpu_reference(A, B, C0, alpha: float, beta: float):
+    """(REF, MAG) as torch FP64 CUDA tensors: alpha*A@B + beta*C0 and
+    |alpha||A||B| + |beta||C0|, for several error checks of one problem."""
     import torch
 
     m, k = A.shape
@@ -154,12 +160,25 @@ def gpu_error_stats(A, B, C0, C, alpha: float, beta: float) -> dict:
     c0 = C0.data_ptr() if C0 is not None else None
     assert gpu().oracle_gpu_dgemm(m, n, k, alpha, A.data_ptr(), A.stride(0), B.data_ptr(),
                                   B.stride(0), beta, c0, n, ref.data_ptr(), mag.data_ptr()) == 0
+    return ref, mag
+
+
+def gpu_error_stats_vs(C, ref, mag) -> dict:
+    """Error statistics of C (torch CUDA FP32) against gpu_reference's output."""
+    m, n = C.shape
     out = np.zeros(5, dtype=np.float64)
     assert gpu().oracle_gpu_error_stats(m, n, C.data_ptr(), C.stride(0), ref.data_ptr(),
                                         mag.data_ptr(), out) == 0
-    del ref, mag
     return {"max_rel": out[0], "mean_rel": out[1], "max_componentwise": out[2],
             "n_rel": int(out[3]), "non_finite": int(out[4])}
+
+
+def gpu_error_stats(A, B, C0, C, alpha: float, beta: float) -> dict:
+    """Full-matrix FP64 error of C (torch CUDA tensors) against alpha*A@B + beta*C0."""
+    ref, mag = gpu_reference(A, B, C0, alpha, beta)
+    out = gpu_error_stats_vs(C, ref, mag)
+    del ref, mag
+    return out
 
 
 # -------------------------------------------------------- reference kernels --
@@ -197,3 +216,32 @@ def ref_sgemm(A, B, C, alpha: float, beta: float, basic: bool = False) -> None:
     f = ref().ref_sgemm_basic if basic else ref().ref_sgemm
     f(m, n, k, ctypes.byref(a), A.data_ptr(), A.stride(0), B.data_ptr(), B.stride(0),
       ctypes.byref(b), C.data_ptr(), C.stride(0))
+
+
+def ref_variant(v: int) -> ctypes.CDLL:
+    """The reference's sgemm() with its PTX macros given a "memory" clobber:
+    v = 1 shared loads, 2 shared stores, 3 every macro."""
+    if v not in _ref_variants:
+        path = os.path.join(HERE, "_ref", f"libref_sgemm_v{v}.so")
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"{path} not built (make -C oracle REF_ROOT=...)")
+        l = ctypes.CDLL(path)
+        fp = ctypes.POINTER(ctypes.c_float)
+        v_ = ctypes.c_void_p
+        l.ref_sgemm.restype = None
+        l.ref_sgemm.argtypes = [_I, _I, _I, fp, v_, _I, v_, _I, fp, v_, _I]
+        l.ref_variant.restype = _I
+        assert l.ref_variant() == v
+        _ref_variants[v] = l
+    return _ref_variants[v]
+
+
+def ref_sgemm_variant(v: int, A, B, C, alpha: float, beta: float) -> None:
+    """Run a clobber variant of the reference's sgemm() on torch CUDA tensors
+    (contiguous, ldb == ldc == n as the reference requires)."""
+    m, k = A.shape
+    n = B.shape[1]
+    a = ctypes.c_float(alpha)
+    b = ctypes.c_float(beta)
+    ref_variant(v).ref_sgemm(m, n, k, ctypes.byref(a), A.data_ptr(), A.stride(0), B.data_ptr(),
+                             B.stride(0), ctypes.byref(b), C.data_ptr(), C.stride(0))

@@ -1,0 +1,94 @@
+// ref_sgemm_variant.cu — TEST INFRASTRUCTURE ONLY.  Builds the reference's
+// own sgemm() (szrlee/sgemm.cu, src/sgemm.cuh:19-48) and its kernels from the
+// reference's unmodified sources, with one change made from the outside: the
+// inline-PTX macros of common/helper_cuda ptx.h are redefined here, before
+// the kernels are included, with a "memory" clobber added.  Nothing of the
+// reference is copied; oracle/Makefile compiles this file with -I pointing at
+// the reference's src/ and common/ and writes oracle/_ref/.
+//
+// Purpose: locate the defect of sgemm_128x128x8 built for sm_100a (wrong
+// results whenever its main loop runs, k > 8).  The reference's macros are
+// `asm volatile` statements with no memory clobber
+// (common/helper_cuda ptx.h:25-40), so the compiler is told that its shared
+// loads (LDS128) and stores (STS128, STS32) touch no memory.  In the main loop
+// (src/kernels/128x128x8.cuh:245-270) the next block's STS and the first
+// fragment loads of that block (LDS128 after the buffer swap) sit on either
+// side of __syncthreads(); a compiler that believes the asm touches no memory
+// may move them across that barrier.  The variants isolate which side:
+//   REF_VARIANT 1: clobber on the shared LOADS only (LDS128)
+//   REF_VARIANT 2: clobber on the shared STORES only (STS128, STS32)
+//   REF_VARIANT 3: clobber on every macro
+// A variant that makes the kernel agree with the oracle bit for bit names the
+// statements the compiler moved.  The benchmark's reference arm never uses
+// these builds; it runs the unmodified reference (ref_sgemm.cu).
+#include "helper_cuda ptx.h"  // the reference's macros; #pragma once keeps them from returning
+
+#ifndef REF_VARIANT
+#error "REF_VARIANT must be 1, 2 or 3"
+#endif
+
+#if REF_VARIANT == 1 || REF_VARIANT == 3
+#undef LDS128_PTX
+#define LDS128_PTX(r0, r1, r2, r3, addr)                                         \
+    { asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];"                      \
+                 : "=f"(r0), "=f"(r1), "=f"(r2), "=f"(r3)                        \
+                 : "l"(addr)                                                     \
+                 : "memory"); }
+#endif
+
+#if REF_VARIANT == 2 || REF_VARIANT == 3
+#undef STS128_PTX
+#define STS128_PTX(r0, r1, r2, r3, addr)                                         \
+    { asm volatile("st.shared.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(addr), "f"(r0), \
+                 "f"(r1), "f"(r2), "f"(r3)                                       \
+                 : "memory"); }
+#undef STS32_PTX
+#define STS32_PTX(r, addr) { asm volatile("st.shared.f32 [%0], %1;" ::"l"(addr), "f"(r) : "memory"); }
+#endif
+
+#if REF_VARIANT == 3
+#undef LDG32_GUARD_PTX
+#define LDG32_GUARD_PTX(r, ptr, guard)                                           \
+    { asm volatile("{.reg .pred q;\n\tsetp.ne.u32 q, %2, 0;\n\t"                   \
+                 "@q ld.global.f32 %0, [%1];}"                                   \
+                 : "=f"(r)                                                       \
+                 : "l"(ptr), "r"(guard)                                          \
+                 : "memory"); }
+#undef LDG32_GUARD_MOV0_PTX
+#define LDG32_GUARD_MOV0_PTX(r, ptr, guard)                                      \
+    { asm volatile("{.reg .pred q;\n\tsetp.ne.u32 q, %2, 0;\n\t"                   \
+                 "@!q mov.b32 %0, 0;\n\t@q ld.global.f32 %0, [%1];}"             \
+                 : "=f"(r)                                                       \
+                 : "l"(ptr), "r"(guard)                                          \
+                 : "memory"); }
+#undef STG32_GUARD_PTX
+#define STG32_GUARD_PTX(r, ptr, guard)                                           \
+    { asm volatile("{.reg .pred q;\n\tsetp.ne.u32 q, %2, 0;\n\t"                   \
+                 "@q st.global.f32 [%0], %1;}" ::"l"(ptr),                       \
+                 "f"(r), "r"(guard)                                              \
+                 : "memory"); }
+#undef CP_ASYNC_GUARD_PTX
+#define CP_ASYNC_GUARD_PTX(saddr, ptr, guard)                                    \
+    { asm volatile("{.reg .pred q;\n\tsetp.ne.u32 q, %2, 0;\n\t"                   \
+                 "@q cp.async.ca.shared.global [%0], [%1], 4;}" ::"l"(saddr),    \
+                 "l"(ptr), "r"(guard)                                            \
+                 : "memory"); }
+#undef CP_ASYNC_IGNORE_SRC_PTX
+#define CP_ASYNC_IGNORE_SRC_PTX(saddr, ptr, guard)                               \
+    { asm volatile("{.reg .pred q;\n\tsetp.eq.u32 q, %2, 0;\n\t"                   \
+                 "cp.async.ca.shared.global [%0], [%1], 4, q;}" ::"l"(saddr),    \
+                 "l"(ptr), "r"(guard)                                            \
+                 : "memory"); }
+#undef WAIT_ALL_PTX
+#define WAIT_ALL_PTX { asm volatile("cp.async.wait_all;" ::: "memory"); }
+#endif
+
+#include <sgemm.cuh>
+
+extern "C" void ref_sgemm(int m, int n, int k, const float* alpha, float* A, int lda, float* B,
+                          int ldb, const float* beta, float* C, int ldc) {
+    sgemm(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+}
+
+extern "C" int ref_variant(void) { return REF_VARIANT; }
+

@@ -107,12 +107,21 @@ bool encode_tensor_map_3d(CUtensorMap* map, CUtensorMapDataType dtype, const voi
     return r == CUDA_SUCCESS;
 }
 
-cudaMemPool_t library_pool() {
-    static cudaMemPool_t pools[kMaxDevices] = {nullptr};
-    static std::mutex mu;
+static cudaMemPool_t g_pools[kMaxDevices] = {nullptr};
+static std::mutex g_pools_mu;
+
+cudaMemPool_t library_pool_if_created() {
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return nullptr;
-    std::lock_guard<std::mutex> lock(mu);
+    std::lock_guard<std::mutex> lock(g_pools_mu);
+    return g_pools[dev];
+}
+
+cudaMemPool_t library_pool() {
+    cudaMemPool_t* pools = g_pools;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return nullptr;
+    std::lock_guard<std::mutex> lock(g_pools_mu);
     if (!pools[dev]) {
         cudaMemPoolProps props;
         std::memset(&props, 0, sizeof(props));
@@ -178,4 +187,20 @@ extern "C" const char* sgemm_b200_status_string(int s) {
     }
 }
 
-extern "C" const char* sgemm_b200_version(void) { return "sgemm_b200 0.1.0 (sm_100a)"; }
+extern "C" const char* sgemm_b200_version(void) { return "sgemm_b200 0.2.0 (sm_100a)"; }
+
+extern "C" int sgemm_b200_abi_version(void) { return SGEMM_B200_ABI_VERSION; }
+
+extern "C" int sgemm_b200_pool_usage(size_t* used_bytes, size_t* reserved_bytes) {
+    if (!used_bytes || !reserved_bytes) return SGEMM_B200_ERR_INVALID_ARG;
+    *used_bytes = *reserved_bytes = 0;
+    cudaMemPool_t p = sgb::library_pool_if_created();  // never creates the pool
+    if (!p) return SGEMM_B200_OK;
+    uint64_t used = 0, reserved = 0;
+    cudaError_t e = cudaMemPoolGetAttribute(p, cudaMemPoolAttrUsedMemCurrent, &used);
+    if (e == cudaSuccess) e = cudaMemPoolGetAttribute(p, cudaMemPoolAttrReservedMemCurrent, &reserved);
+    if (e != cudaSuccess) return sgb::cuda_status(e);
+    *used_bytes = (size_t)used;
+    *reserved_bytes = (size_t)reserved;
+    return SGEMM_B200_OK;
+}

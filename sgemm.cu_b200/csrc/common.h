@@ -57,6 +57,9 @@ bool encode_tensor_map_3d(CUtensorMap* map, CUtensorMapDataType dtype, const voi
 // unlimited, so freed blocks are reused by the next call instead of going back
 // to the driver; the caller's default pool is left untouched.
 cudaMemPool_t library_pool();
+// The current device's library pool if a call has created it, else null
+// (never creates it).
+cudaMemPool_t library_pool_if_created();
 
 // Shape checks common to every entry point.  Returns SGEMM_B200_OK or
 // SGEMM_B200_ERR_INVALID_ARG.

@@ -331,14 +331,21 @@ extern "C" int sgemm_b200_config_count(void) { return sgb::plain_config_count();
 
 extern "C" const char* sgemm_b200_config_name(int cfg) { return sgb::plain_config_name(cfg); }
 
-extern "C" int sgemm_b200_select_config(int m, int n, int k, const float* A, int lda,
-                                        const float* B, int ldb, const float* beta) {
+extern "C" int sgemm_b200_select_config_beta(int m, int n, int k, const float* A, int lda,
+                                             const float* B, int ldb, const float* beta) {
     if (m <= 0 || n <= 0 || k < 0) return -1;
     const bool reads_c = beta == nullptr || *beta != 0.0f;
     // the kernel that runs: after a pack step the operands are TMA-aligned
     if (sgb::ffma::pack_mask(m, n, k, A, lda, B, ldb))
         return sgb::select_for_loader(m, n, k, sgb::ffma::kLoaderTma, reads_c);
     return sgb::plain_select(m, n, k, A, lda, B, ldb, reads_c);
+}
+
+extern "C" int sgemm_b200_select_config(int m, int n, int k, const float* A, int lda,
+                                        const float* B, int ldb, const float* C, int ldc) {
+    (void)C;
+    (void)ldc;
+    return sgemm_b200_select_config_beta(m, n, k, A, lda, B, ldb, nullptr);
 }
 
 extern "C" int sgemm_b200_packs(int m, int n, int k, const float* A, int lda, const float* B,

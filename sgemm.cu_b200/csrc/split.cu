@@ -597,10 +597,15 @@ extern "C" int sgemm_b200_gemm(int path, int m, int n, int k, const float* alpha
 // pre-pass writes) is a file-scope static device array of kNoAllocScratchBytes,
 // so the call itself never allocates.  The array is created when this
 // library's device code is loaded on a GPU and stays until the process exits.
+// It holds 64 MiB of planes plus the 1 KiB a workspace reserves to align its
+// base, so a problem fits exactly when sgemm_b200_split_workspace_size() is at
+// most kNoAllocScratchBytes: up to m = n = k = 2048 for TF32X3 (planes of
+// exactly 64 MiB) and 2361 for BF16X6.
 namespace sgb {
 namespace noalloc {
 
-constexpr size_t kNoAllocScratchBytes = size_t(64) << 20;  // 64 MiB per GPU
+constexpr size_t kNoAllocPlaneBytes = size_t(64) << 20;              // 64 MiB of planes
+constexpr size_t kNoAllocScratchBytes = kNoAllocPlaneBytes + 1024;  // + base alignment
 static __device__ __align__(256) uint8_t g_split_scratch[kNoAllocScratchBytes];
 
 constexpr int kMaxDevices = 64;

@@ -97,6 +97,9 @@ class TraceRecord(ctypes.Structure):
 
 _lib: Optional[ctypes.CDLL] = None
 
+# The C ABI version this binding was written against (SGEMM_B200_ABI_VERSION).
+ABI_VERSION = 2
+
 _I = ctypes.c_int
 _P = ctypes.c_void_p
 _FP = ctypes.POINTER(ctypes.c_float)
@@ -113,7 +116,9 @@ def _declare(lib: ctypes.CDLL) -> None:
     d("sgemm_b200_with_config", _I, [_I] + _GEMM_ARGS + [_P])
     d("sgemm_b200_config_count", _I, [])
     d("sgemm_b200_config_name", ctypes.c_char_p, [_I])
-    d("sgemm_b200_select_config", _I, [_I, _I, _I, _P, _I, _P, _I, _FP])
+    d("sgemm_b200_select_config", _I, [_I, _I, _I, _P, _I, _P, _I, _P, _I])
+    d("sgemm_b200_select_config_beta", _I, [_I, _I, _I, _P, _I, _P, _I, _FP])
+    d("sgemm_b200_abi_version", _I, [])
     d("sgemm_b200_packs", _I, [_I, _I, _I, _P, _I, _P, _I])
     d("sgemm_b200_basic", _I, _GEMM_ARGS + [_P])
     d("sgemm_b200_split_workspace_size", ctypes.c_size_t, [_I, _I, _I, _I])
@@ -138,6 +143,8 @@ def _declare(lib: ctypes.CDLL) -> None:
     d("sgemm_b200_autotune_grouped", _I, [ctypes.POINTER(Problem), _I, ctypes.c_char_p])
     d("sgemm_b200_fill_random", _I, [_P, _I, _I, _I, ctypes.c_uint64, ctypes.c_uint32, _I, _P])
     d("sgemm_b200_device_status", _I, [])
+    d("sgemm_b200_pool_usage", _I, [ctypes.POINTER(ctypes.c_size_t),
+                                     ctypes.POINTER(ctypes.c_size_t)])
     d("sgemm_b200_selftest_wait_timeout", _I, [_I, _P])
     d("sgemm_b200_last_status", _I, [])
     d("sgemm_b200_status_string", ctypes.c_char_p, [_I])
@@ -179,6 +186,9 @@ def lib() -> ctypes.CDLL:
                 "(or __graft_entry__.build()); there is no fallback path")
         l = ctypes.CDLL(LIB_PATH)
         _declare(l)
+        if l.sgemm_b200_abi_version() != ABI_VERSION:
+            raise ImportError(f"{LIB_PATH} has C ABI version {l.sgemm_b200_abi_version()}, this "
+                              f"binding needs {ABI_VERSION}: rebuild the library")
         _lib = l
     return _lib
 
@@ -325,8 +335,8 @@ def select_config(m: int, n: int, k: int, A=None, lda: int = 0, B=None, ldb: int
     this beta (None: C is read)."""
     pa = A.data_ptr() if A is not None else 16
     pb = B.data_ptr() if B is not None else 16
-    return lib().sgemm_b200_select_config(m, n, k, pa, lda or k, pb, ldb or n,
-                                          None if beta is None else _f(beta))
+    return lib().sgemm_b200_select_config_beta(m, n, k, pa, lda or k, pb, ldb or n,
+                                               None if beta is None else _f(beta))
 
 
 def packs(m: int, n: int, k: int, A=None, lda: int = 0, B=None, ldb: int = 0) -> int:
@@ -344,6 +354,14 @@ def selftest_wait_timeout(limit_us: int, stream=None) -> None:
 
 def device_status() -> int:
     return lib().sgemm_b200_device_status()
+
+
+def pool_usage() -> tuple:
+    """(used, reserved) bytes of the library's own memory pool on the current
+    device; (0, 0) before any call has created it."""
+    u, r = ctypes.c_size_t(), ctypes.c_size_t()
+    _check(lib().sgemm_b200_pool_usage(ctypes.byref(u), ctypes.byref(r)), "pool_usage")
+    return u.value, r.value
 
 
 def make_problems(specs: Sequence) -> "ctypes.Array":

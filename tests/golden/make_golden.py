@@ -7,8 +7,9 @@ oracle/_ref/libref_sgemm.so by oracle/Makefile -- on inputs from the oracle's
 seeded generator, and stores the outputs as raw float32 files plus index.json.
 tests/test_oracle.py then pins the CPU oracle to these outputs.
 
-Needs a B200.  Usage:  python tests/golden/make_golden.py OUT_DIR
-(copy OUT_DIR/* into tests/golden/ afterwards).
+Needs a B200.  Usage:  python tests/golden/make_golden.py [OUT_DIR]
+(default: a new temporary directory, printed at the end; copy OUT_DIR/* into
+tests/golden/ afterwards).
 """
 import hashlib
 import json
@@ -75,4 +76,8 @@ def main(out_dir: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else os.path.join(ROOT, "gpurun_out", "golden"))
+    import tempfile
+
+    out = sys.argv[1] if len(sys.argv) > 1 else tempfile.mkdtemp(prefix="sgemm_golden_")
+    main(out)
+    print(f"fixtures written to {out}")

@@ -87,18 +87,32 @@ def test_config_table():
     l = sg.lib()
     # unaligned strides: small problems run a cp.async configuration in place;
     # from 512^3 the offending operands are packed and a TMA configuration runs
-    c = l.sgemm_b200_select_config(300, 301, 299, 16, 299, 16, 301, None)
+    c = l.sgemm_b200_select_config_beta(300, 301, 299, 16, 299, 16, 301, None)
     assert names[c].startswith("cpa_") and l.sgemm_b200_packs(300, 301, 299, 16, 299, 16, 301) == 0
-    c = l.sgemm_b200_select_config(3001, 3001, 3001, 16, 3001, 16, 3001, None)
+    c = l.sgemm_b200_select_config_beta(3001, 3001, 3001, 16, 3001, 16, 3001, None)
     assert names[c].startswith("tma_") and l.sgemm_b200_packs(3001, 3001, 3001, 16, 3001, 16,
                                                               3001) == 3
     assert l.sgemm_b200_packs(3001, 3000, 3001, 16, 3001, 16, 3000) == 1  # A only
     assert l.sgemm_b200_packs(3000, 3001, 3000, 16, 3000, 16, 3001) == 2  # B only
     assert l.sgemm_b200_packs(3001, 3001, 3001, 16, 3004, 16, 3004) == 0  # padded pitches
     assert l.sgemm_b200_packs(3000, 3000, 3000, 20, 3000, 16, 3000) == 1  # A base not 16-aligned
-    c = l.sgemm_b200_select_config(8192, 8192, 8192, 16, 8192, 16, 8192, None)
+    c = l.sgemm_b200_select_config_beta(8192, 8192, 8192, 16, 8192, 16, 8192, None)
     assert names[c].startswith("tma_") and l.sgemm_b200_packs(8192, 8192, 8192, 16, 8192, 16,
                                                               8192) == 0
+
+
+def test_select_config_keeps_its_first_signature():
+    # sgemm_b200_select_config(m, n, k, A, lda, B, ldb, C, ldc) is the form the
+    # first release exported; the beta-aware query is a separate entry point,
+    # and the ABI version tells callers which header the library matches.
+    l = sg.lib()
+    assert l.sgemm_b200_abi_version() == sg.ABI_VERSION == 2
+    for shape in ((300, 301, 299), (1024, 1024, 1024), (8192, 8192, 8192)):
+        m, n, k = shape
+        old = l.sgemm_b200_select_config(m, n, k, 16, k, 16, n, 16, n)
+        assert old == l.sgemm_b200_select_config_beta(m, n, k, 16, k, 16, n, None)
+        assert old == l.sgemm_b200_select_config_beta(m, n, k, 16, k, 16, n,
+                                                      ctypes.byref(ctypes.c_float(0.5)))
 
 
 def test_host_entry_validation_and_bands():

@@ -3,10 +3,12 @@
 That entry point is for callers that may not allocate device memory inside a
 call (a framework that owns the GPU's allocator, latency-critical loops where
 cudaMalloc/cudaFree would synchronise the device, fixed-footprint
-deployments).  Its scratch is one static 64 MiB device array inside the
-library, shared by every call.  This test calls it through the C ABI and
-checks it against the allocating entry point, sgemm_b200_split, on two calls
-in a row: the second call runs on whatever the first left in the shared array.
+deployments).  Its scratch is one static device array inside the library
+(64 MiB of operand planes plus 1 KiB of alignment), shared by every call.
+These tests call it through the C ABI and check it against the allocating
+entry point, sgemm_b200_split, on two calls in a row (the second call runs on
+whatever the first left in the shared array), check that a call allocates
+nothing, and check the size limit on both sides.
 The file is named to be collected last.
 """
 import ctypes
@@ -65,6 +67,84 @@ def test_noalloc_matches_allocating_entry_point_twice(path):
         e = oracle.error_stats(got, ref, mag)
         ep = oracle.error_stats(oracle.sgemm_basic(A, B, C, 1.5, 0.5, basic=False), ref, mag)
         assert e["max_componentwise"] <= 1.5 * ep["max_componentwise"] + 2.0 ** -23
+
+
+def _memory_state():
+    import torch
+
+    torch.cuda.synchronize()
+    return sg.pool_usage(), torch.cuda.mem_get_info()[0], torch.cuda.memory_allocated()
+
+
+@pytest.mark.parametrize("path", ["bf16x6", "tf32x3"])
+def test_noalloc_allocates_nothing(path):
+    """The property that defines the entry point: a call leaves the library's
+    own pool, torch's allocator and the device's free memory as they were.
+    A first call is made before measuring, so that one-time costs that are not
+    allocations by the call (loading the kernels' code onto the device, the
+    symbol lookup) do not show; the k == 0 and beta == 0 routes are covered."""
+    import torch
+
+    m, n, k = 640, 384, 1000
+    A = oracle.fill(m, k, 41, 1, 0)
+    B = oracle.fill(k, n, 41, 2, 0)
+    C = oracle.fill(m, n, 41, 3, 0)
+    dA, dB = torch.from_numpy(A).cuda(), torch.from_numpy(B).cuda()
+    outs = [torch.from_numpy(C).cuda() for _ in range(4)]
+    assert _call_noalloc(path, dA, dB, outs[0], 1.5, 0.5) == sg.OK  # warm-up
+    before = _memory_state()
+    assert _call_noalloc(path, dA, dB, outs[1], 1.5, 0.5) == sg.OK
+    assert _call_noalloc(path, dA, dB, outs[2], 1.0, 0.0) == sg.OK  # beta == 0: C not read
+    # k == 0: C := beta * C, no planes
+    assert _call_noalloc(path, dA[:, :0], dB[:0, :], outs[3], 1.5, 0.5) == sg.OK
+    after = _memory_state()
+    assert sg.device_status() == sg.OK
+    assert after == before, f"memory changed across the calls: {before} -> {after}"
+    # the results of those calls: beta == 0 against the allocating entry point
+    # (C filled with NaN, which must never be read), k == 0 against the oracle
+    nan_c = torch.full((m, n), float("nan"), device="cuda")
+    assert _call_noalloc(path, dA, dB, nan_c, 1.0, 0.0) == sg.OK
+    want = torch.from_numpy(C).cuda()
+    sg.sgemm_split(path, dA, dB, want, 1.0, 0.0)
+    torch.cuda.synchronize()
+    assert torch.equal(outs[2], want) and torch.equal(nan_c, want)
+    want_k0 = oracle.sgemm_basic(np.zeros((m, 0), np.float32), np.zeros((0, n), np.float32), C,
+                                 1.5, 0.5, basic=False)
+    assert np.array_equal(outs[3].cpu().numpy(), want_k0)
+    assert torch.equal(outs[0], outs[1])
+
+
+@pytest.mark.parametrize("path,largest", [("bf16x6", 2361), ("tf32x3", 2048)])
+def test_noalloc_size_boundary(path, largest):
+    """The largest accepted cube runs and equals the allocating entry point;
+    one more row, column or k step is refused before any work."""
+    import torch
+
+    p = sg.PATHS[path]
+    limit = (64 << 20) + 1024
+    assert sg.split_workspace_size(p, largest, largest, largest) <= limit
+    n = largest
+    A = torch.empty((n, n), device="cuda")
+    B = torch.empty((n, n), device="cuda")
+    C0 = torch.empty((n, n), device="cuda")
+    for t, X in ((1, A), (2, B), (3, C0)):
+        sg.fill_random(X, 43, t, sg.DIST_UNIFORM_PM1)
+    c_new, c_old = C0.clone(), C0.clone()
+    assert _call_noalloc(path, A, B, c_new, 1.5, 0.5) == sg.OK
+    sg.sgemm_split(path, A, B, c_old, 1.5, 0.5)
+    torch.cuda.synchronize()
+    assert sg.device_status() == sg.OK
+    assert torch.equal(c_new, c_old)
+    # k is padded to a multiple of 8, so the next larger k is 8 more
+    for dm, dn, dk in ((1, 0, 0), (0, 1, 0), (0, 0, 8)):
+        m2, n2, k2 = n + dm, n + dn, n + dk
+        assert sg.split_workspace_size(p, m2, n2, k2) > limit
+        A2 = torch.zeros((m2, k2), device="cuda")
+        B2 = torch.zeros((k2, n2), device="cuda")
+        C2 = torch.full((m2, n2), 7.0, device="cuda")
+        assert _call_noalloc(path, A2, B2, C2, 1.0, 0.0) == sg.ERR_NO_MEMORY
+        torch.cuda.synchronize()
+        assert bool((C2 == 7.0).all())  # nothing ran
 
 
 def test_noalloc_refuses_problems_beyond_its_scratch():
