@@ -571,6 +571,21 @@ def _grouped_leg(torch, sg, sms, sm_mhz, hbm_gbs, count=512):
     t_tuned = timed(lambda: plan.launch(use_graph=True), 7)
     tinfo = plan.info()
     plan.close()
+    # the same 512 problems on the split-precision path: one grouped pre-pass +
+    # one persistent tcgen05 launch, against one sgemm_b200_split call each
+    split = {}
+    for name in ("bf16x6", "tf32x3"):
+        try:
+            t_gs = timed(lambda: sg.grouped_split(name, probs), 5)
+            t_ss = timed(lambda: sg.grouped_split_sequential(name, probs), 3)
+            split[name] = {"grouped_ms": round(t_gs, 3),
+                           "grouped_gflops": round(flop / t_gs * 1e-6, 1),
+                           "sequential_ms": round(t_ss, 3),
+                           "sequential_gflops": round(flop / t_ss * 1e-6, 1),
+                           "speedup_vs_sequential": round(t_ss / t_gs, 3),
+                           "launches": 2, "sequential_launches": 3 * len(shapes)}
+        except Exception as e:  # report, never hide
+            split[name] = {"error": str(e)}
     with open(tuned) as f:
         table = json.load(f)
     os.unlink(tuned)
@@ -595,6 +610,7 @@ def _grouped_leg(torch, sg, sms, sm_mhz, hbm_gbs, count=512):
         "launches": 1, "tiles": info["tiles"], "work_items_default": info["work_items"],
         "work_items_tuned": tinfo["work_items"], "autotune_s": round(tune_s, 1),
         "tuning": table,
+        "split_paths": split,
     }
 
 
@@ -612,18 +628,33 @@ def _serving_bounds(sg, path, rate, n_requests, seed, simt_gflops, tc_useful_gfl
     return sum(flops) / sum(gaps[1:]) * 1e-9, sum(flops) / roof_s * 1e-9
 
 
+def _pct(xs, q):
+    """Nearest-rank percentile."""
+    xs = sorted(xs)
+    return xs[min(len(xs) - 1, max(0, int(np.ceil(q * len(xs))) - 1))]
+
+
 def _serving_leg(sg, rates, n_requests, simt_gflops, tc_useful_gflops, hbm_gbs):
     out = {"workload": "Poisson arrivals; 60% M~U[16,256] N=K=4096, 40% M=N=K log-uniform "
                        "[512,4096]; operands generated and resident on the device; 64 GB "
                        "budget; 2 slots, max batch 32; each server first serves 32 untimed "
                        "warm-up requests (first-use costs: staging buffers, kernel loads)",
-           "runs": []}
+           "requests_per_rate": n_requests, "runs": []}
     for path in ("plain", "bf16x6"):
+        srv = sg.Server(64 << 30, slots=2, max_batch=32, path=path)
+        srv.run_poisson(rates[0], 32, seed=7)  # warm-up; the next run starts fresh stats
+        # each distinct request shape served alone through this server's own
+        # launch path: the floor its latency is compared with (the shapes do not
+        # depend on the rate, only the arrival gaps do)
+        shapes, _ = sg.serving_workload(n_requests, rates[0], 11)
+        iso = {sh: srv.isolated_ms(*sh, reps=3) for sh in sorted(set(shapes))}
         for rate in rates:
-            srv = sg.Server(64 << 30, slots=2, max_batch=32, path=path)
-            srv.run_poisson(rate, 32, seed=7)  # warm-up; the next run starts fresh stats
             st = srv.run_poisson(rate, n_requests, seed=11)
-            srv.close()
+            trace = srv.trace()
+            lat = [r["done_ms"] - r["submit_ms"] for r in trace]
+            slow = [(r["done_ms"] - r["submit_ms"]) / iso[(r["m"], r["n"], r["k"])]
+                    for r in trace]
+            iso_req = [iso[(r["m"], r["n"], r["k"])] for r in trace]
             offered, roof = _serving_bounds(sg, path, rate, n_requests, 11, simt_gflops,
                                             tc_useful_gflops, hbm_gbs)
             out["runs"].append({
@@ -632,13 +663,23 @@ def _serving_leg(sg, rates, n_requests, simt_gflops, tc_useful_gflops, hbm_gbs):
                 "p99_ms": round(st["p99_ms"], 3),
                 "queue_p99_ms": round(st["queue_p99_ms"], 3),
                 "service_p99_ms": round(st["service_p99_ms"], 3),
+                "isolated_p50_ms": round(_pct(iso_req, 0.5), 3),
+                "isolated_p99_ms": round(_pct(iso_req, 0.99), 3),
+                "slowdown_p50": round(_pct(slow, 0.5), 2),
+                "slowdown_p99": round(_pct(slow, 0.99), 2),
+                "traced": len(lat),
                 "gflops": round(st["gflops"], 1),
                 "batches": st["batches"], "max_batch": st["max_batch_size"],
                 "max_batches_in_flight": st["max_batches_in_flight"],
                 "offered_gflops": round(offered, 1), "roofline_gflops": round(roof, 1),
-                "frac_of_bound": round(st["gflops"] / min(offered, roof), 4)})
-    out["bound_note"] = ("frac_of_bound = achieved GFLOP/s / min(offered load, roofline of the "
-                         "mix); below saturation the offered load is the bound")
+                "achieved_over_roofline": round(st["gflops"] / roof, 4),
+                "saturated": bool(st["gflops"] < 0.97 * offered)})
+        srv.close()
+    out["bound_note"] = ("slowdown = a request's latency (submit to completion) / its shape's "
+                         "device time served alone through the same server path (isolated); "
+                         "achieved_over_roofline = achieved GFLOP/s / the mix's roofline (each "
+                         "request at the path's compute peak or HBM bandwidth, whichever binds); "
+                         "below saturation achieved equals the offered load")
     return out
 
 
@@ -800,7 +841,8 @@ def run(args):
                                          args.grouped_problems)
         torch.cuda.empty_cache()
     if rank == 0 and world == 1 and not args.skip_serving:
-        result["serving"] = _serving_leg(sg, [500.0, 1000.0, 2000.0, 4000.0], 300,
+        result["serving"] = _serving_leg(sg, [500.0, 1000.0, 2000.0, 4000.0],
+                                         args.serving_requests,
                                          sms * 256 * sm_max * 1e-3,
                                          peaks["bf16_tflops"] * 1e3 / 6, peaks["hbm_gbs"])
     if rank == 0:
@@ -897,6 +939,8 @@ def main():
                     help="skip the cuBLAS / library tensor-core context numbers")
     ap.add_argument("--skip-grouped", action="store_true")
     ap.add_argument("--skip-serving", action="store_true")
+    ap.add_argument("--serving-requests", type=int, default=3000,
+                    help="requests per serving run (default 3000)")
     ap.add_argument("--grouped-problems", type=int, default=512,
                     help="problems in the grouped leg (default 512; fewer only for profiler "
                          "captures)")

@@ -293,6 +293,24 @@ int sgemm_b200_grouped_schedule(const sgemm_b200_problem* problems, int count,
                                 const char* tuning_json, int* tiles, int* work_items,
                                 size_t* workspace_bytes);
 
+/* Grouped split-precision GEMM (no reference counterpart): every problem of
+ * the table -- C := alpha*A*B + beta*C, each with sgemm_b200's argument
+ * meaning -- through one grouped pre-pass launch that writes all problems'
+ * BF16 (path BF16X6) or TF32 (path TF32X3) planes, and one launch of a
+ * persistent tcgen05 kernel over the 128 x 256 tiles of all problems
+ * (per-problem tensor maps, longest tiles first).  Each problem's result
+ * equals sgemm_b200_split's on its own, bit for bit.  Workspace for the
+ * planes and the launch tables come stream-ordered from the library's pool
+ * and are released after the kernels.  Problems with k == 0 run on the plain
+ * path (C := beta*C).  Stream-ordered; returns without synchronising. */
+int sgemm_b200_grouped_split(int path, const sgemm_b200_problem* problems, int count,
+                             sgemm_b200_stream_t stream);
+
+/* The baseline that launch replaces: one sgemm_b200_split call per problem,
+ * in order, on `stream`. */
+int sgemm_b200_grouped_split_sequential(int path, const sgemm_b200_problem* problems, int count,
+                                        sgemm_b200_stream_t stream);
+
 /* Size bucket (0..8) the tuning table keys a problem by: 3 classes of M*N
  * (< 256^2, < 1024^2, larger) x 3 classes of K (< 512, < 2048, larger). */
 int sgemm_b200_grouped_bucket(int m, int n, int k);

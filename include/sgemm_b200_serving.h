@@ -3,21 +3,31 @@
  * counterpart: the reference has no serving code).
  *
  * A server owns one device memory pool of `hbm_budget_bytes`.  Each request
- * is a GEMM C := alpha*A*B + beta*C whose operands the server allocates from
- * the pool when the request is admitted and keeps resident on the device
- * until the caller releases the request.  Admission is by memory: a request
- * waits in the arrival queue until its A, B and C fit in the pool, and is
- * refused (SGEMM_B200_ERR_REJECTED) if they could never fit.
+ * is a GEMM C := alpha*A*B + beta*C.  Its operands come from one of three
+ * places, chosen by the submit call:
+ *   - sgemm_b200_server_submit_device: the caller's own device matrices,
+ *     used in place (the result lands in the caller's C);
+ *   - sgemm_b200_server_submit_host: the caller's host matrices, copied into
+ *     the pool when the request is admitted and C copied back after its batch,
+ *     both inside the request's latency;
+ *   - sgemm_b200_server_submit: matrices the server generates in the pool from
+ *     a seed (for load tests that need no caller data).
+ * Pool memory -- operands held in the pool, and the split paths' workspace --
+ * is allocated when the request is admitted and kept until the request
+ * completes (or, with keep_results, until the caller releases it).  Admission
+ * is by memory: a request waits in the arrival queue until its pool memory
+ * fits, and is refused (SGEMM_B200_ERR_REJECTED) if it could never fit.
  *
  * Continuous batching: admitted requests are grouped into batches as soon as
- * one of `slots` CUDA streams is free; each batch runs as one launch of the
- * persistent grouped kernel (plain path) or as one split-precision GEMM per
- * request (BF16X6 / TF32X3 paths) on that slot's stream.  Requests that
+ * one of `slots` CUDA streams is free; each batch runs on that slot's stream
+ * as one launch of the persistent grouped FFMA kernel (plain path) or as one
+ * grouped split pre-pass plus one launch of the persistent grouped tcgen05
+ * kernel (BF16X6 / TF32X3 paths).  Requests that
  * arrive while other batches are on the GPU are admitted as memory frees and
  * join the next batch, so batches overlap on the device.  Every request's
  * result is independent of the batch it lands in: the grouped kernel runs
- * the plain path's exact arithmetic per problem, and the split paths compute
- * each request alone.
+ * the plain path's exact arithmetic per problem, and the grouped split kernel
+ * computes each tile exactly as the single split GEMM does.
  *
  * Latency of a request = completion minus submission, on the host's steady
  * clock.  Completion is when the server's completion thread, which polls an
@@ -92,14 +102,50 @@ void sgemm_b200_server_destroy(sgemm_b200_server* server);
 int sgemm_b200_server_submit(sgemm_b200_server* server, int m, int n, int k, float alpha,
                              float beta, uint64_t seed, int64_t* request_id);
 
+/* Submit C := alpha*A*B + beta*C on the caller's DEVICE matrices (on the
+ * server's device; row-major, row strides lda >= k, ldb >= n, ldc >= n, the
+ * meaning of sgemm_b200's arguments).  The matrices must be complete on the
+ * device when this is called (the server does not wait on the caller's
+ * streams).  Ownership stays with the caller: A and B must stay valid and
+ * unchanged, and C must be neither read nor written, until the request has
+ * completed (sgemm_b200_server_wait or _drain); C is then the result.  The
+ * pool holds only the split paths' workspace.  Returns at once. */
+int sgemm_b200_server_submit_device(sgemm_b200_server* server, int m, int n, int k,
+                                    float alpha, const float* A, int lda, const float* B,
+                                    int ldb, float beta, float* C, int ldc,
+                                    int64_t* request_id);
+
+/* Submit C := alpha*A*B + beta*C on the caller's HOST matrices (row-major,
+ * strides as above).  At admission the server allocates A, B and C in its
+ * pool and copies A, B (and C when beta != 0) in on its ingest stream; after
+ * the request's batch it copies C back into the caller's C.  The request
+ * completes when that copy has landed, so its latency includes both copies.
+ * The buffers must stay valid and unchanged (C untouched) until completion;
+ * page-locked memory lets the copies run asynchronously (pageable memory
+ * works, but each copy then blocks the server's worker thread while it runs).
+ * Returns at once. */
+int sgemm_b200_server_submit_host(sgemm_b200_server* server, int m, int n, int k, float alpha,
+                                  const float* A, int lda, const float* B, int ldb, float beta,
+                                  float* C, int ldc, int64_t* request_id);
+
+/* Block until one request has completed, failed or been refused; returns
+ * SGEMM_B200_OK, SGEMM_B200_ERR_CUDA or SGEMM_B200_ERR_REJECTED and, when
+ * completed, its latency.  Must not race with sgemm_b200_server_release of the
+ * same request. */
+int sgemm_b200_server_wait(sgemm_b200_server* server, int64_t request_id, double* latency_ms);
+
 /* Block until every submitted request has completed or been refused. */
 int sgemm_b200_server_drain(sgemm_b200_server* server);
 
-/* Result of a completed request (keep_results != 0): latency and the device
- * pointer of its C (row stride n), valid until released. */
+/* Result of a completed request: latency and the device pointer and row
+ * stride of its C -- the caller's own C for device requests, else the pool's
+ * copy (kept only with keep_results != 0, valid until released; NULL once
+ * the pool memory has been freed). */
 int sgemm_b200_server_result(sgemm_b200_server* server, int64_t request_id, double* latency_ms,
                              const float** C, int* ldc, int* batch_size);
-/* Copy a completed request's C (m x n, row-major, packed) to host memory. */
+/* Copy a completed request's C (m x n) to host memory as packed rows: from
+ * the device C (device requests, or pool copies that are kept) or from the
+ * caller's host C (host requests). */
 int sgemm_b200_server_read_result(sgemm_b200_server* server, int64_t request_id, float* host_out);
 int sgemm_b200_server_release(sgemm_b200_server* server, int64_t request_id);
 
@@ -111,6 +157,16 @@ int sgemm_b200_server_get_stats(sgemm_b200_server* server, sgemm_b200_server_sta
  * later completions still count in the statistics but are not traced. */
 int sgemm_b200_server_get_trace(sgemm_b200_server* server, sgemm_b200_server_trace_record* out,
                                 int max, int* count);
+
+/* Device time of one request of shape m x n x k served alone through this
+ * server's own batch launch (the same kernels, on one of its slot streams,
+ * operands generated in its pool): the median of `reps` launches, as the
+ * device span the trace records for served batches.  The server must be idle
+ * (nothing queued or running, else SGEMM_B200_ERR_INVALID_ARG), and the
+ * request's pool memory must fit (else SGEMM_B200_ERR_NO_MEMORY).  Used as the
+ * floor a served request's latency is compared with. */
+int sgemm_b200_server_isolated_ms(sgemm_b200_server* server, int m, int n, int k, int reps,
+                                  double* ms);
 
 /* Open-loop load: `n_requests` requests with exponential inter-arrival times
  * of mean 1/rate_per_s; 60% tall-skinny (M uniform in [16, 256], N = K =

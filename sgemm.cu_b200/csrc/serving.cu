@@ -8,8 +8,9 @@
 //  - one worker thread admits requests in arrival order while their operands
 //    fit in the pool (generating them on an ingest stream), forms a batch
 //    whenever one of `slots` streams is free, and launches it: one persistent
-//    grouped kernel (plain path) or one split GEMM per request (split paths),
-//    followed by an event on the slot's stream;
+//    grouped FFMA kernel (plain path) or one grouped split pre-pass and one
+//    persistent grouped tcgen05 kernel (split paths), followed by an event on
+//    the slot's stream;
 //  - one completion thread polls the events of the batches in flight
 //    (cudaEventQuery, about every 20 us, asleep while nothing is in flight),
 //    stamps the completion time of a finished batch's requests and hands the
@@ -23,6 +24,7 @@
 #include <chrono>
 #include <cmath>
 #include <condition_variable>
+#include <cstring>
 #include <deque>
 #include <map>
 #include <mutex>
@@ -34,6 +36,7 @@
 #include "common.h"
 #include "grouped.h"
 #include "rng.h"
+#include "split.h"
 
 // ------------------------------------------------------------------- pool --
 
@@ -127,14 +130,27 @@ static double secs(Clock::time_point t) {
 
 enum ReqState { kWaiting, kAdmitted, kRunning, kDone, kRejected, kFailed };
 
+// Where a request's operands come from:
+//  kGenerated  the server generates them in its pool (seeded, uniform[-1, 1))
+//  kDevice     the caller's device matrices, used in place (C written in place)
+//  kHost       the caller's host matrices: copied into the pool at admission,
+//              C copied back after the batch (both inside the request's latency)
+enum ReqKind { kGenerated = 0, kDevice = 1, kHost = 2 };
+
 struct Request {
     int64_t id = 0;
+    int kind = kGenerated;
     int m = 0, n = 0, k = 0;
+    int lda = 0, ldb = 0, ldc = 0;  // of A, B, C as the kernels read them
     float alpha = 1, beta = 0;
     uint64_t seed = 0;
     size_t bytes = 0, ws_bytes = 0;
     int64_t off = -1;
-    float *A = nullptr, *B = nullptr, *C = nullptr;
+    float *A = nullptr, *B = nullptr, *C = nullptr;  // device operands the batch uses
+    const float* hA = nullptr;                       // kHost: the caller's buffers
+    const float* hB = nullptr;
+    float* hC = nullptr;
+    int h_lda = 0, h_ldb = 0, h_ldc = 0;
     void* ws = nullptr;
     double t_submit = 0, t_admit = 0, t_launch = 0, t_done = 0;
     int state = kWaiting;
@@ -150,7 +166,8 @@ struct Slot {
     bool error = false;  // the batch's end event reported an error
     bool busy = false;
     std::vector<Request*> batch;
-    grouped::Arena arena;
+    grouped::Arena arena;      // plain path: grouped FFMA launches
+    split::Arena split_arena;  // split paths: grouped tcgen05 launches
 };
 
 struct Server;
@@ -227,12 +244,14 @@ static void completer_loop(Server* s) {
     }
 }
 
-static size_t request_bytes(int path, int m, int n, int k, size_t* ws) {
+// Pool bytes of one request: its operands (unless they are the caller's
+// device matrices) and the split workspace.
+static size_t request_bytes(int path, int kind, int m, int n, int k, size_t* ws) {
     const size_t a = round_up((size_t)m * k * 4), b = round_up((size_t)k * n * 4),
                  c = round_up((size_t)m * n * 4);
     *ws = path == SGEMM_B200_PATH_PLAIN ? 0
                                         : round_up(sgemm_b200_split_workspace_size(path, m, n, k));
-    return a + b + c + *ws;
+    return (kind == kDevice ? 0 : a + b + c) + *ws;
 }
 
 // Called with the lock held.
@@ -284,6 +303,7 @@ static void finish_slot(Server* s, int si) {
     sl.busy = false;
     sl.error = false;
     --s->in_flight;
+    s->cv_drain.notify_all();  // sgemm_b200_server_wait waits for single requests
 }
 
 // Admit arrivals in order while they fit (called with the lock held).
@@ -310,20 +330,37 @@ static void admit(Server* s) {
         uint8_t* base = s->d_pool + off;
         const size_t a = round_up((size_t)r->m * r->k * 4), b = round_up((size_t)r->k * r->n * 4),
                      c = round_up((size_t)r->m * r->n * 4);
-        r->A = reinterpret_cast<float*>(base);
-        r->B = reinterpret_cast<float*>(base + a);
-        r->C = reinterpret_cast<float*>(base + a + b);
-        r->ws = r->ws_bytes ? base + a + b + c : nullptr;
         s->peak_pool = std::max(s->peak_pool, s->pool.used);
-        // Operands arrive: generated on the device, resident from here on.
-        sgemm_b200_fill_random(r->A, r->m, r->k, r->k, r->seed, 1, SGEMM_B200_DIST_UNIFORM_PM1,
-                               s->ingest);
-        sgemm_b200_fill_random(r->B, r->k, r->n, r->n, r->seed, 2, SGEMM_B200_DIST_UNIFORM_PM1,
-                               s->ingest);
-        sgemm_b200_fill_random(r->C, r->m, r->n, r->n, r->seed, 3, SGEMM_B200_DIST_UNIFORM_PM1,
-                               s->ingest);
-        cudaEventCreateWithFlags(&r->ready, cudaEventDisableTiming);
-        cudaEventRecord(r->ready, s->ingest);
+        if (r->kind == kDevice) {
+            // The caller's matrices, complete on the device before submission:
+            // nothing to wait for (ready stays null).
+            r->ws = r->ws_bytes ? base : nullptr;
+        } else {
+            r->A = reinterpret_cast<float*>(base);
+            r->B = reinterpret_cast<float*>(base + a);
+            r->C = reinterpret_cast<float*>(base + a + b);
+            r->ws = r->ws_bytes ? base + a + b + c : nullptr;
+            if (r->kind == kGenerated) {
+                // Operands arrive: generated on the device, resident from here on.
+                sgemm_b200_fill_random(r->A, r->m, r->k, r->k, r->seed, 1,
+                                       SGEMM_B200_DIST_UNIFORM_PM1, s->ingest);
+                sgemm_b200_fill_random(r->B, r->k, r->n, r->n, r->seed, 2,
+                                       SGEMM_B200_DIST_UNIFORM_PM1, s->ingest);
+                sgemm_b200_fill_random(r->C, r->m, r->n, r->n, r->seed, 3,
+                                       SGEMM_B200_DIST_UNIFORM_PM1, s->ingest);
+            } else {
+                // The caller's host matrices cross into the pool (C only if read).
+                cudaMemcpy2DAsync(r->A, (size_t)r->k * 4, r->hA, (size_t)r->h_lda * 4,
+                                  (size_t)r->k * 4, r->m, cudaMemcpyHostToDevice, s->ingest);
+                cudaMemcpy2DAsync(r->B, (size_t)r->n * 4, r->hB, (size_t)r->h_ldb * 4,
+                                  (size_t)r->n * 4, r->k, cudaMemcpyHostToDevice, s->ingest);
+                if (r->beta != 0.0f)
+                    cudaMemcpy2DAsync(r->C, (size_t)r->n * 4, r->hC, (size_t)r->h_ldc * 4,
+                                      (size_t)r->n * 4, r->m, cudaMemcpyHostToDevice, s->ingest);
+            }
+            cudaEventCreateWithFlags(&r->ready, cudaEventDisableTiming);
+            cudaEventRecord(r->ready, s->ingest);
+        }
         r->t_admit = secs(Clock::now());
         r->state = kAdmitted;
         s->ready.push_back(r);
@@ -358,22 +395,38 @@ static int launch_batch(Server* s, int si) {
     Slot& sl = s->slots[si];
     if (s->cfg.inject_batch_delay_ms > 0)
         std::this_thread::sleep_for(std::chrono::milliseconds(s->cfg.inject_batch_delay_ms));
-    for (Request* r : sl.batch) cudaStreamWaitEvent(sl.stream, r->ready, 0);
+    for (Request* r : sl.batch)
+        if (r->ready) cudaStreamWaitEvent(sl.stream, r->ready, 0);
     int st = cuda_status(cudaEventRecord(sl.ev_start, sl.stream));
     if (st == SGEMM_B200_OK && s->cfg.path == SGEMM_B200_PATH_PLAIN) {
         std::vector<sgemm_b200_problem> probs(sl.batch.size());
         for (size_t i = 0; i < sl.batch.size(); ++i) {
             const Request* r = sl.batch[i];
-            probs[i] = sgemm_b200_problem{r->m, r->n, r->k, r->k, r->n, r->n, r->alpha,
-                                          r->beta, r->A, r->B, r->C};
+            probs[i] = sgemm_b200_problem{r->m,     r->n,    r->k, r->lda, r->ldb, r->ldc,
+                                          r->alpha, r->beta, r->A, r->B,   r->C};
         }
         st = grouped::arena_launch(&sl.arena, probs.data(), (int)probs.size(), sl.stream);
     } else if (st == SGEMM_B200_OK) {
-        for (Request* r : sl.batch) {
-            st = sgemm_b200_split(s->cfg.path, r->m, r->n, r->k, &r->alpha, r->A, r->k, r->B,
-                                  r->n, &r->beta, r->C, r->n, r->ws, r->ws_bytes, sl.stream);
-            if (st != SGEMM_B200_OK) break;
+        // one grouped pre-pass and one persistent tcgen05 launch for the batch
+        std::vector<sgemm_b200_problem> probs(sl.batch.size());
+        std::vector<void*> ws(sl.batch.size());
+        for (size_t i = 0; i < sl.batch.size(); ++i) {
+            const Request* r = sl.batch[i];
+            probs[i] = sgemm_b200_problem{r->m,     r->n,    r->k, r->lda, r->ldb, r->ldc,
+                                          r->alpha, r->beta, r->A, r->B,   r->C};
+            ws[i] = r->ws;
         }
+        st = split::grouped_launch(&sl.split_arena, s->cfg.path, probs.data(), ws.data(),
+                                   (int)probs.size(), sl.stream);
+    }
+    // Results the caller wants in host memory go back before the batch counts
+    // as complete.
+    for (Request* r : sl.batch) {
+        if (st != SGEMM_B200_OK) break;
+        if (r->kind == kHost)
+            st = cuda_status(cudaMemcpy2DAsync(r->hC, (size_t)r->h_ldc * 4, r->C, (size_t)r->ldc * 4,
+                                               (size_t)r->n * 4, r->m, cudaMemcpyDeviceToHost,
+                                               sl.stream));
     }
     if (st == SGEMM_B200_OK) st = cuda_status(cudaEventRecord(sl.ev_end, sl.stream));
     return st;
@@ -409,7 +462,7 @@ static void worker_loop(Server* s) {
             const bool gpu_idle = s->in_flight == 0;
             while (!s->ready.empty() && (int)sl.batch.size() < s->cfg.max_batch) {
                 Request* r = s->ready.front();
-                if (!gpu_idle && cudaEventQuery(r->ready) == cudaErrorNotReady) break;
+                if (!gpu_idle && r->ready && cudaEventQuery(r->ready) == cudaErrorNotReady) break;
                 s->ready.pop_front();
                 r->state = kRunning;
                 sl.batch.push_back(r);
@@ -460,7 +513,7 @@ static void worker_loop(Server* s) {
             }
             continue;
         }
-        if (s->outstanding == 0) s->cv_drain.notify_all();
+        s->cv_drain.notify_all();  // drain and per-request waiters re-check
         if (s->stop && s->outstanding == 0) break;
         if (wait_for_operands)
             s->cv.wait_for(lock, std::chrono::microseconds(20));
@@ -546,19 +599,13 @@ extern "C" int sgemm_b200_server_create(sgemm_b200_server** out,
     return SGEMM_B200_OK;
 }
 
-extern "C" int sgemm_b200_server_submit(sgemm_b200_server* srv, int m, int n, int k, float alpha,
-                                        float beta, uint64_t seed, int64_t* id) {
-    if (!srv || m <= 0 || n <= 0 || k <= 0) return SGEMM_B200_ERR_INVALID_ARG;
-    Server* s = &srv->s;
-    auto* r = new Request();
-    r->m = m;
-    r->n = n;
-    r->k = k;
-    r->alpha = alpha;
-    r->beta = beta;
-    r->seed = seed;
-    r->bytes = sgb::serving::request_bytes(s->cfg.path, m, n, k, &r->ws_bytes);
-    r->t_submit = sgb::serving::secs(sgb::serving::Clock::now());
+namespace sgb {
+namespace serving {
+
+// Queue a filled-in request (shape, kind, operands); assigns its id.
+static int submit(Server* s, Request* r, int64_t* id) {
+    r->bytes = request_bytes(s->cfg.path, r->kind, r->m, r->n, r->k, &r->ws_bytes);
+    r->t_submit = secs(Clock::now());
     std::lock_guard<std::mutex> lock(s->mu);
     r->auto_release = s->cfg.keep_results == 0;
     r->id = s->next_id++;
@@ -570,7 +617,7 @@ extern "C" int sgemm_b200_server_submit(sgemm_b200_server* srv, int m, int n, in
         s->epoch_set = cudaEventRecord(s->epoch, s->ingest) == cudaSuccess;
     }
     if (r->bytes > s->pool.capacity) {  // could never fit: refuse now
-        r->state = sgb::serving::kRejected;
+        r->state = kRejected;
         ++s->rejected;
         return SGEMM_B200_ERR_REJECTED;
     }
@@ -578,6 +625,91 @@ extern "C" int sgemm_b200_server_submit(sgemm_b200_server* srv, int m, int n, in
     s->arrivals.push_back(r);
     s->cv.notify_all();
     return SGEMM_B200_OK;
+}
+
+}  // namespace serving
+}  // namespace sgb
+
+extern "C" int sgemm_b200_server_submit(sgemm_b200_server* srv, int m, int n, int k, float alpha,
+                                        float beta, uint64_t seed, int64_t* id) {
+    if (!srv || m <= 0 || n <= 0 || k <= 0) return SGEMM_B200_ERR_INVALID_ARG;
+    auto* r = new Request();
+    r->kind = sgb::serving::kGenerated;
+    r->m = m;
+    r->n = n;
+    r->k = k;
+    r->lda = k;
+    r->ldb = n;
+    r->ldc = n;
+    r->alpha = alpha;
+    r->beta = beta;
+    r->seed = seed;
+    return sgb::serving::submit(&srv->s, r, id);
+}
+
+extern "C" int sgemm_b200_server_submit_device(sgemm_b200_server* srv, int m, int n, int k,
+                                               float alpha, const float* A, int lda,
+                                               const float* B, int ldb, float beta, float* C,
+                                               int ldc, int64_t* id) {
+    if (!srv || m <= 0 || n <= 0 || k <= 0 || !A || !B || !C || lda < k || ldb < n || ldc < n)
+        return SGEMM_B200_ERR_INVALID_ARG;
+    auto* r = new Request();
+    r->kind = sgb::serving::kDevice;
+    r->m = m;
+    r->n = n;
+    r->k = k;
+    r->lda = lda;
+    r->ldb = ldb;
+    r->ldc = ldc;
+    r->alpha = alpha;
+    r->beta = beta;
+    r->A = const_cast<float*>(A);
+    r->B = const_cast<float*>(B);
+    r->C = C;
+    return sgb::serving::submit(&srv->s, r, id);
+}
+
+extern "C" int sgemm_b200_server_submit_host(sgemm_b200_server* srv, int m, int n, int k,
+                                             float alpha, const float* A, int lda, const float* B,
+                                             int ldb, float beta, float* C, int ldc,
+                                             int64_t* id) {
+    if (!srv || m <= 0 || n <= 0 || k <= 0 || !A || !B || !C || lda < k || ldb < n || ldc < n)
+        return SGEMM_B200_ERR_INVALID_ARG;
+    auto* r = new Request();
+    r->kind = sgb::serving::kHost;
+    r->m = m;
+    r->n = n;
+    r->k = k;
+    r->lda = k;  // packed in the pool
+    r->ldb = n;
+    r->ldc = n;
+    r->alpha = alpha;
+    r->beta = beta;
+    r->hA = A;
+    r->hB = B;
+    r->hC = C;
+    r->h_lda = lda;
+    r->h_ldb = ldb;
+    r->h_ldc = ldc;
+    return sgb::serving::submit(&srv->s, r, id);
+}
+
+extern "C" int sgemm_b200_server_wait(sgemm_b200_server* srv, int64_t id, double* latency_ms) {
+    if (!srv) return SGEMM_B200_ERR_INVALID_ARG;
+    Server* s = &srv->s;
+    std::unique_lock<std::mutex> lock(s->mu);
+    auto it = s->all.find(id);
+    if (it == s->all.end()) return SGEMM_B200_ERR_INVALID_ARG;
+    Request* r = it->second;
+    s->cv.notify_all();
+    s->cv_drain.wait(lock, [&] {
+        return r->state == sgb::serving::kDone || r->state == sgb::serving::kFailed ||
+               r->state == sgb::serving::kRejected;
+    });
+    if (latency_ms) *latency_ms = (r->t_done - r->t_submit) * 1e3;
+    return r->state == sgb::serving::kDone       ? SGEMM_B200_OK
+           : r->state == sgb::serving::kRejected ? SGEMM_B200_ERR_REJECTED
+                                                 : SGEMM_B200_ERR_CUDA;
 }
 
 extern "C" int sgemm_b200_server_drain(sgemm_b200_server* srv) {
@@ -600,8 +732,10 @@ extern "C" int sgemm_b200_server_result(sgemm_b200_server* srv, int64_t id, doub
     if (r->state == sgb::serving::kRejected) return SGEMM_B200_ERR_REJECTED;
     if (r->state != sgb::serving::kDone) return SGEMM_B200_ERR_CUDA;
     if (latency_ms) *latency_ms = (r->t_done - r->t_submit) * 1e3;
-    if (C) *C = r->off >= 0 ? r->C : nullptr;
-    if (ldc) *ldc = r->n;
+    // the caller's own C (device requests), else the pool's copy while it is kept
+    const bool device_c = r->kind == sgb::serving::kDevice || r->off >= 0;
+    if (C) *C = device_c ? r->C : nullptr;
+    if (ldc) *ldc = r->ldc;
     if (batch_size) *batch_size = r->batch_size;
     return SGEMM_B200_OK;
 }
@@ -610,19 +744,33 @@ extern "C" int sgemm_b200_server_read_result(sgemm_b200_server* srv, int64_t id,
     if (!srv || !host_out) return SGEMM_B200_ERR_INVALID_ARG;
     Server* s = &srv->s;
     const float* C = nullptr;
-    int m = 0, n = 0;
+    const float* hC = nullptr;
+    int m = 0, n = 0, ldc = 0;
     {
         std::lock_guard<std::mutex> lock(s->mu);
         auto it = s->all.find(id);
         if (it == s->all.end()) return SGEMM_B200_ERR_INVALID_ARG;
         Request* r = it->second;
-        if (r->state != sgb::serving::kDone || r->off < 0) return SGEMM_B200_ERR_INVALID_ARG;
-        C = r->C;
+        if (r->state != sgb::serving::kDone) return SGEMM_B200_ERR_INVALID_ARG;
         m = r->m;
         n = r->n;
+        if (r->kind == sgb::serving::kHost) {
+            hC = r->hC;  // the result is already in the caller's host C
+            ldc = r->h_ldc;
+        } else {
+            if (r->kind == sgb::serving::kGenerated && r->off < 0)
+                return SGEMM_B200_ERR_INVALID_ARG;  // released with its pool memory
+            C = r->C;
+            ldc = r->ldc;
+        }
     }
-    return sgb::cuda_status(
-        cudaMemcpy(host_out, C, sizeof(float) * (size_t)m * n, cudaMemcpyDeviceToHost));
+    if (hC) {
+        for (int i = 0; i < m; ++i)
+            std::memcpy(host_out + (size_t)i * n, hC + (size_t)i * ldc, sizeof(float) * n);
+        return SGEMM_B200_OK;
+    }
+    return sgb::cuda_status(cudaMemcpy2D(host_out, sizeof(float) * n, C, sizeof(float) * ldc,
+                                         sizeof(float) * n, m, cudaMemcpyDeviceToHost));
 }
 
 extern "C" int sgemm_b200_server_release(sgemm_b200_server* srv, int64_t id) {
@@ -639,6 +787,75 @@ extern "C" int sgemm_b200_server_release(sgemm_b200_server* srv, int64_t id) {
     delete r;
     s->all.erase(it);
     s->cv.notify_all();
+    return SGEMM_B200_OK;
+}
+
+extern "C" int sgemm_b200_server_isolated_ms(sgemm_b200_server* srv, int m, int n, int k,
+                                             int reps, double* ms) {
+    if (!srv || !ms || m <= 0 || n <= 0 || k <= 0 || reps < 1) return SGEMM_B200_ERR_INVALID_ARG;
+    Server* s = &srv->s;
+    Request r;
+    r.kind = sgb::serving::kGenerated;
+    r.m = m;
+    r.n = n;
+    r.k = k;
+    r.lda = k;
+    r.ldb = n;
+    r.ldc = n;
+    r.alpha = 1.0f;
+    r.beta = 0.0f;
+    r.bytes = sgb::serving::request_bytes(s->cfg.path, r.kind, m, n, k, &r.ws_bytes);
+    int si = -1;
+    {
+        // Take a free slot while nothing is queued or running, so the
+        // measurement has the GPU to itself and the worker leaves the slot alone.
+        std::lock_guard<std::mutex> lock(s->mu);
+        if (s->outstanding != 0 || s->in_flight != 0) return SGEMM_B200_ERR_INVALID_ARG;
+        for (size_t i = 0; i < s->slots.size(); ++i)
+            if (!s->slots[i].busy) {
+                si = (int)i;
+                break;
+            }
+        if (si < 0) return SGEMM_B200_ERR_INVALID_ARG;
+        r.off = sgb::serving::pool_alloc(&s->pool, r.bytes);
+        if (r.off < 0) return SGEMM_B200_ERR_NO_MEMORY;
+        s->slots[si].busy = true;
+    }
+    sgb::serving::Slot& sl = s->slots[si];
+    uint8_t* base = s->d_pool + r.off;
+    const size_t a = sgb::serving::round_up((size_t)m * k * 4),
+                 b = sgb::serving::round_up((size_t)k * n * 4),
+                 c = sgb::serving::round_up((size_t)m * n * 4);
+    r.A = reinterpret_cast<float*>(base);
+    r.B = reinterpret_cast<float*>(base + a);
+    r.C = reinterpret_cast<float*>(base + a + b);
+    r.ws = r.ws_bytes ? base + a + b + c : nullptr;
+    int st = sgemm_b200_fill_random(r.A, m, k, k, 1, 1, SGEMM_B200_DIST_UNIFORM_PM1, sl.stream);
+    if (st == SGEMM_B200_OK)
+        st = sgemm_b200_fill_random(r.B, k, n, n, 1, 2, SGEMM_B200_DIST_UNIFORM_PM1, sl.stream);
+    std::vector<float> t;
+    sl.batch.assign(1, &r);
+    // one untimed launch, then `reps` timed ones: the batch's device span, as
+    // the trace records it for served batches
+    for (int i = 0; i <= reps && st == SGEMM_B200_OK; ++i) {
+        st = sgb::serving::launch_batch(s, si);
+        if (st == SGEMM_B200_OK) st = sgb::cuda_status(cudaEventSynchronize(sl.ev_end));
+        float x = 0;
+        if (st == SGEMM_B200_OK && i > 0)
+            st = sgb::cuda_status(cudaEventElapsedTime(&x, sl.ev_start, sl.ev_end));
+        if (i > 0) t.push_back(x);
+    }
+    if (st != SGEMM_B200_OK) cudaStreamSynchronize(sl.stream);
+    {
+        std::lock_guard<std::mutex> lock(s->mu);
+        sl.batch.clear();
+        sl.busy = false;
+        sgb::serving::pool_free(&s->pool, r.off);
+        s->cv.notify_all();
+    }
+    if (st != SGEMM_B200_OK) return st;
+    std::sort(t.begin(), t.end());
+    *ms = t[t.size() / 2];
     return SGEMM_B200_OK;
 }
 
@@ -762,6 +979,7 @@ extern "C" void sgemm_b200_server_destroy(sgemm_b200_server* srv) {
         if (sl.stream) cudaStreamSynchronize(sl.stream);
     for (auto& sl : s->slots) {
         sgb::grouped::arena_release(&sl.arena);
+        sgb::split::arena_release(&sl.split_arena);
         if (sl.stream) cudaStreamDestroy(sl.stream);
         if (sl.ev_start) cudaEventDestroy(sl.ev_start);
         if (sl.ev_end) cudaEventDestroy(sl.ev_end);

@@ -40,13 +40,16 @@
 // transposed to [split][N][Kp], both K-major) into a workspace.
 #include <cuda_bf16.h>
 
+#include <algorithm>
 #include <atomic>
 #include <cstring>
 #include <mutex>
+#include <vector>
 
 #include "common.h"
 #include "plain.h"
 #include "ptx.cuh"
+#include "split.h"
 
 namespace sgb {
 namespace split {
@@ -389,36 +392,42 @@ __device__ __forceinline__ void store8(uint8_t* plane0, int64_t plane_bytes, int
     }
 }
 
-// A [m x lda] -> planes [split][m][kp], zero in columns k..kp-1.  One thread
-// per 8 consecutive k of one row.
+// A [m x lda] -> planes [split][m][kp], zero in columns k..kp-1: chunk i of
+// the m * kp/8 chunks is 8 consecutive k of one row.
 template <int PATH>
-__global__ void split_a_kernel(const float* __restrict__ A, int m, int k, int lda, int kp,
-                               uint8_t* __restrict__ out) {
+__device__ __forceinline__ void split_a_chunk(const float* __restrict__ A, int m, int k, int lda,
+                                              int kp, uint8_t* __restrict__ out, int64_t i) {
     using T = Traits<PATH>;
     const int64_t plane_bytes = (int64_t)m * kp * T::ESZ;
     const int chunks = kp / 8;
-    const int64_t total = (int64_t)m * chunks;
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
-         i += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t r = i / chunks;
-        const int c0 = (int)(i % chunks) * 8;
-        float v[8][3];
+    const int64_t r = i / chunks;
+    const int c0 = (int)(i % chunks) * 8;
+    float v[8][3];
 #pragma unroll
-        for (int j = 0; j < 8; ++j) {
-            const float x = c0 + j < k ? A[r * lda + c0 + j] : 0.0f;
-            split_value<PATH>(x, v[j]);
-        }
-        store8<PATH>(out, plane_bytes, r * kp + c0, v);
+    for (int j = 0; j < 8; ++j) {
+        const float x = c0 + j < k ? A[r * lda + c0 + j] : 0.0f;
+        split_value<PATH>(x, v[j]);
     }
+    store8<PATH>(out, plane_bytes, r * kp + c0, v);
 }
 
-// B [k x ldb] -> transposed planes [split][n][kp] via 64 x 64 shared tiles.
 template <int PATH>
-__global__ void split_bt_kernel(const float* __restrict__ B, int k, int n, int ldb, int kp,
-                                uint8_t* __restrict__ out) {
+__global__ void split_a_kernel(const float* __restrict__ A, int m, int k, int lda, int kp,
+                               uint8_t* __restrict__ out) {
+    const int64_t total = (int64_t)m * (kp / 8);
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
+         i += (int64_t)gridDim.x * blockDim.x)
+        split_a_chunk<PATH>(A, m, k, lda, kp, out, i);
+}
+
+// B [k x ldb] -> transposed planes [split][n][kp]: one 64 (k) x 64 (n) tile
+// (bx along n, by along k) through shared memory, by a block of 256 threads.
+template <int PATH>
+__device__ __forceinline__ void split_bt_tile(const float* __restrict__ B, int k, int n, int ldb,
+                                              int kp, uint8_t* __restrict__ out, int bx, int by,
+                                              float (&tile)[64][65]) {
     using T = Traits<PATH>;
-    __shared__ float tile[64][65];
-    const int k0 = blockIdx.y * 64, n0 = blockIdx.x * 64;
+    const int k0 = by * 64, n0 = bx * 64;
     const int tx = threadIdx.x % 64, ty = threadIdx.x / 64;  // 256 threads
 #pragma unroll 4
     for (int i = 0; i < 16; ++i) {
@@ -438,6 +447,13 @@ __global__ void split_bt_kernel(const float* __restrict__ B, int k, int n, int l
         for (int j = 0; j < 8; ++j) split_value<PATH>(tile[kc + j][nn], v[j]);
         store8<PATH>(out, plane_bytes, (int64_t)gn * kp + gk, v);
     }
+}
+
+template <int PATH>
+__global__ void split_bt_kernel(const float* __restrict__ B, int k, int n, int ldb, int kp,
+                                uint8_t* __restrict__ out) {
+    __shared__ float tile[64][65];
+    split_bt_tile<PATH>(B, k, n, ldb, kp, out, blockIdx.x, blockIdx.y, tile);
 }
 
 template <int PATH>
@@ -524,6 +540,570 @@ static int launch(int m, int n, int k, float alpha, const float* A, int lda, con
     return cuda_status(cudaGetLastError());
 }
 
+// ------------------------------------------------------- grouped split GEMM --
+//
+// Many split-precision problems in two launches: one pre-pass that writes
+// every problem's planes, and one persistent tcgen05 kernel over the tiles of
+// all problems.  Per problem: two tensor maps (A planes, B planes) in global
+// memory, and its own epilogue scalars.  Each tile is computed exactly as
+// split_gemm_kernel computes it (same planes, same MMA order, same K chunks of
+// D1, same epilogue), so every problem's result equals sgemm_b200_split's bit
+// for bit, whatever else is in the launch.
+//
+// Persistent schedule: CTA c of G takes, in round r, the tile at position
+// r*G + c (r even) or r*G + G-1-c (r odd) of a list sorted longest first (the
+// snake order pairs long and short tiles).  Every role of the CTA walks the
+// same sequence, so no tile index needs to pass between warps.  Across tiles
+// the roles keep running counts (k blocks through the stage ring, D1 chunks)
+// for mbarrier phases, and one more barrier, d2_empty, lets the MMA warp
+// overwrite D2 for the next tile only after the drain warps have read it.
+
+struct GSProblem {
+    int m, n, k, ldc;
+    float alpha, beta;
+    float* C;
+    int vec_c, pad;
+};
+
+struct GSTile {
+    int prob, tm, tn, nk;
+};
+
+struct GSParams {
+    const GSProblem* probs;
+    const GSTile* tiles;
+    const CUtensorMap* maps;  // 2 per problem: A planes, B planes
+    int* status;
+    int n_tiles;
+};
+
+__device__ __forceinline__ int snake_tile(int c, int r, int G) {
+    return r * G + ((r & 1) ? (G - 1 - c) : c);
+}
+
+template <int PATH>
+__global__ void __maxnreg__(200) split_grouped_kernel(const GSParams gp) {
+    using T = Traits<PATH>;
+    using L = Layout<PATH>;
+    extern __shared__ uint8_t smem_raw[];
+    __shared__ __align__(8) uint64_t full_bar[T::STAGES];
+    __shared__ __align__(8) uint64_t empty_bar[T::STAGES];
+    __shared__ __align__(8) uint64_t d1_full_bar;
+    __shared__ __align__(8) uint64_t d1_empty_bar;
+    __shared__ __align__(8) uint64_t d2_empty_bar;
+    __shared__ uint32_t tmem_base_s;
+    __shared__ volatile int abort_s;
+    __shared__ uint32_t consumed_s;
+    uint8_t* smem = align_smem_1024(smem_raw);
+
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int G = gridDim.x, cta = blockIdx.x;
+
+    if (tid == 0) {
+        for (int s = 0; s < T::STAGES; ++s) {
+            mbar_init(&full_bar[s], 1);
+            mbar_init(&empty_bar[s], 1);
+        }
+        mbar_init(&d1_full_bar, 1);
+        mbar_init(&d1_empty_bar, DRAIN_WARPS);
+        mbar_init(&d2_empty_bar, DRAIN_WARPS);
+        abort_s = 0;
+        consumed_s = 0;
+        fence_barrier_init();
+    }
+    if (warp == 0) {
+        tmem_alloc(&tmem_base_s, TMEM_COLS);
+        tmem_relinquish();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = tmem_base_s;
+
+    uint32_t issued = 0;
+    if (warp == PRODUCER_WARP) {
+        if (lane == 0) {
+            // ------------------------------------------------ TMA producer --
+            uint32_t g = 0;  // k blocks issued through the stage ring
+            bool ok = true;
+            for (int r = 0; ok && r * G < gp.n_tiles; ++r) {
+                const int t = snake_tile(cta, r, G);
+                if (t >= gp.n_tiles) continue;
+                const GSTile tl = gp.tiles[t];
+                const CUtensorMap* tmA = gp.maps + 2 * tl.prob;
+                const CUtensorMap* tmB = tmA + 1;
+                tma_prefetch_desc(tmA);
+                tma_prefetch_desc(tmB);
+                for (int kb = 0; kb < tl.nk; ++kb, ++g) {
+                    const int s = g % T::STAGES;
+                    if (g >= (uint32_t)T::STAGES) {
+                        if (!mbar_wait(&empty_bar[s], ((g / T::STAGES) - 1) & 1) || abort_s) {
+                            abort_s = 1;
+                            atomicExch(gp.status, SGEMM_B200_ERR_TIMEOUT);
+                            ok = false;
+                            break;
+                        }
+                    }
+                    uint8_t* st = smem + s * L::STAGE_BYTES;
+                    mbar_arrive_expect_tx(&full_bar[s], L::STAGE_BYTES);
+                    tma_load_3d(st, tmA, &full_bar[s], kb * T::BK, tl.tm * BM, 0);
+                    tma_load_3d(st + L::A_BYTES, tmB, &full_bar[s], kb * T::BK, tl.tn * BN, 0);
+                    ++issued;
+                }
+            }
+        }
+    } else if (warp == MMA_WARP) {
+        if (lane == 0) {
+            // -------------------------------------------------- MMA issuer --
+            constexpr uint32_t idesc = make_idesc(T::FMT, BM, BN);
+            const uint32_t d1 = tmem, d2 = tmem + static_cast<uint32_t>(BN);
+            uint32_t g = 0;   // k blocks consumed
+            uint32_t cg = 0;  // D1 chunks committed
+            int it = 0;       // tiles begun by this CTA
+            bool ok = true;
+            for (int r = 0; ok && r * G < gp.n_tiles; ++r) {
+                const int t = snake_tile(cta, r, G);
+                if (t >= gp.n_tiles) continue;
+                const GSTile tl = gp.tiles[t];
+                const int nsteps = tl.nk * L::STEPS;
+                if (it > 0) {  // D2 of the previous tile must be read before it is reset
+                    if (!mbar_wait(&d2_empty_bar, (it - 1) & 1) || abort_s) {
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                }
+                for (int kb = 0; kb < tl.nk; ++kb, ++g) {
+                    const int s = g % T::STAGES;
+                    if (!mbar_wait(&full_bar[s], (g / T::STAGES) & 1) || abort_s) {
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t a0 = smem_u32(smem + s * L::STAGE_BYTES);
+                    const uint32_t b0 = a0 + L::A_BYTES;
+#pragma unroll
+                    for (int j = 0; j < L::STEPS; ++j) {
+                        const int step = kb * L::STEPS + j;
+                        const uint32_t koff = j * T::KMMA * T::ESZ;
+#pragma unroll
+                        for (int i = 0; i < T::NPROD - 1; ++i) {
+                            const uint64_t ad =
+                                sw64_kmajor_desc(a0 + T::pa(i) * L::A_PLANE + koff);
+                            const uint64_t bd =
+                                sw64_kmajor_desc(b0 + T::pb(i) * L::B_PLANE + koff);
+                            const uint32_t accum = (step > 0 || i > 0) ? 1u : 0u;
+                            if constexpr (T::FMT == 1)
+                                mma_bf16_ss(d2, ad, bd, idesc, accum);
+                            else
+                                mma_tf32_ss(d2, ad, bd, idesc, accum);
+                        }
+                        const bool chunk_start = step % L::CHUNK_STEPS == 0;
+                        if (chunk_start && cg > 0) {
+                            if (!mbar_wait(&d1_empty_bar, (cg - 1) & 1) || abort_s) {
+                                ok = false;
+                                break;
+                            }
+                            tc_fence_after();
+                        }
+                        {
+                            const int i = T::NPROD - 1;
+                            const uint64_t ad =
+                                sw64_kmajor_desc(a0 + T::pa(i) * L::A_PLANE + koff);
+                            const uint64_t bd =
+                                sw64_kmajor_desc(b0 + T::pb(i) * L::B_PLANE + koff);
+                            if constexpr (T::FMT == 1)
+                                mma_bf16_ss(d1, ad, bd, idesc, chunk_start ? 0u : 1u);
+                            else
+                                mma_tf32_ss(d1, ad, bd, idesc, chunk_start ? 0u : 1u);
+                        }
+                        if ((step + 1) % L::CHUNK_STEPS == 0 || step + 1 == nsteps) {
+                            mma_commit(&d1_full_bar);
+                            ++cg;
+                        }
+                    }
+                    if (!ok) break;
+                    mma_commit(&empty_bar[s]);
+                }
+                ++it;
+            }
+            if (!ok) {
+                abort_s = 1;
+                atomicExch(gp.status, SGEMM_B200_ERR_TIMEOUT);
+            }
+            consumed_s = g;
+        }
+    } else {
+        // ------------------------------------------------ drain + epilogue --
+        const int q = warp & 3, h = warp >> 2;
+        const uint32_t trow = tmem + (static_cast<uint32_t>(q * 32) << 16) + h * 128;
+        uint32_t cg = 0;
+        int it = 0;
+        bool ok = true;
+        for (int r = 0; ok && r * G < gp.n_tiles; ++r) {
+            const int t = snake_tile(cta, r, G);
+            if (t >= gp.n_tiles) continue;
+            const GSTile tl = gp.tiles[t];
+            const int nchunks = (tl.nk * L::STEPS + L::CHUNK_STEPS - 1) / L::CHUNK_STEPS;
+            float acc[128];
+#pragma unroll
+            for (int j = 0; j < 128; ++j) acc[j] = 0.0f;
+            for (int c = 0; c < nchunks; ++c, ++cg) {
+                if (!mbar_wait(&d1_full_bar, cg & 1) || abort_s) {
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+#pragma unroll
+                for (int gq = 0; gq < 4; ++gq) {
+                    uint32_t rr[32];
+                    tmem_ld_32x32b_x32(trow + gq * 32, rr);
+                    tmem_ld_wait();
+#pragma unroll
+                    for (int j = 0; j < 32; ++j)
+                        acc[gq * 32 + j] = __fadd_rn(acc[gq * 32 + j], __uint_as_float(rr[j]));
+                }
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&d1_empty_bar);
+            }
+            if (!ok || abort_s) break;
+            // D2 is complete (the tile's last D1 commit came after its MMAs):
+            // read it all, release it to the MMA warp, then store C.  The
+            // outputs replace the running sums in place (acc doubles as v).
+            float(&v)[128] = acc;
+            const float alpha = gp.probs[tl.prob].alpha;
+#pragma unroll
+            for (int gq = 0; gq < 4; ++gq) {
+                uint32_t rr[32];
+                tmem_ld_32x32b_x32(trow + BN + gq * 32, rr);
+                tmem_ld_wait();
+#pragma unroll
+                for (int j = 0; j < 32; ++j)
+                    v[gq * 32 + j] =
+                        __fmul_rn(__fadd_rn(acc[gq * 32 + j], __uint_as_float(rr[j])), alpha);
+            }
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&d2_empty_bar);
+            const GSProblem& p = gp.probs[tl.prob];
+            const int row = tl.tm * BM + q * 32 + lane;
+#pragma unroll
+            for (int gq = 0; gq < 4; ++gq) {
+                const int col0 = tl.tn * BN + h * 128 + gq * 32;
+                if (row >= p.m || col0 >= p.n) continue;
+                float* crow = p.C + (int64_t)row * p.ldc + col0;
+                if (p.vec_c && col0 + 31 < p.n) {
+#pragma unroll
+                    for (int u = 0; u < 8; ++u) {
+                        float4 o = make_float4(v[gq * 32 + 4 * u], v[gq * 32 + 4 * u + 1],
+                                               v[gq * 32 + 4 * u + 2], v[gq * 32 + 4 * u + 3]);
+                        float4* dst = reinterpret_cast<float4*>(crow + 4 * u);
+                        if (p.beta != 0.0f) {
+                            const float4 old = *dst;
+                            o.x = fmaf(old.x, p.beta, o.x);
+                            o.y = fmaf(old.y, p.beta, o.y);
+                            o.z = fmaf(old.z, p.beta, o.z);
+                            o.w = fmaf(old.w, p.beta, o.w);
+                        }
+                        *dst = o;
+                    }
+                } else {
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) {
+                        if (col0 + j < p.n) {
+                            float o = v[gq * 32 + j];
+                            if (p.beta != 0.0f) o = fmaf(crow[j], p.beta, o);
+                            crow[j] = o;
+                        }
+                    }
+                }
+            }
+            ++it;
+        }
+        if (!ok) {
+            abort_s = 1;
+            atomicExch(gp.status, SGEMM_B200_ERR_TIMEOUT);
+        }
+    }
+
+    // ------------------------------------------------------------ teardown --
+    tc_fence_before();
+    __syncthreads();
+    if (warp == PRODUCER_WARP && lane == 0) {
+        // Copies the MMA issuer never consumed (only after an abort) must land
+        // before this CTA's shared memory is released.
+        for (uint32_t j = consumed_s; j < issued; ++j)
+            if (!mbar_wait(&full_bar[j % T::STAGES], (j / T::STAGES) & 1)) break;
+    }
+    if (warp == 0) {
+        __syncwarp();
+        tmem_dealloc(tmem, TMEM_COLS);
+    }
+}
+
+// Grouped pre-pass: the A and B planes of many problems in one launch.
+// Blocks [0, a_blocks) split A chunks (256 chunks of 8 k-values per block),
+// blocks [a_blocks, a_blocks + b_blocks) transpose-and-split 64 x 64 tiles of
+// B; a block finds its problem by binary search over the prefix sums.
+struct PrepJob {
+    const float* A;
+    const float* B;
+    uint8_t* wa;
+    uint8_t* wb;
+    int m, n, k, kp, lda, ldb;
+    int b_tiles_n;  // 64-column tiles of B along n
+    int pad;
+};
+
+struct PrepParams {
+    const PrepJob* jobs;
+    const int* a_prefix;  // n_jobs + 1 entries
+    const int* b_prefix;
+    int n_jobs;
+    int a_blocks;
+};
+
+template <int PATH>
+__global__ void __launch_bounds__(256) split_prepass_grouped_kernel(const PrepParams pp) {
+    __shared__ float tile[64][65];
+    int b = blockIdx.x;
+    const bool is_a = b < pp.a_blocks;
+    const int* pref = is_a ? pp.a_prefix : pp.b_prefix;
+    if (!is_a) b -= pp.a_blocks;
+    int lo = 0, hi = pp.n_jobs - 1;  // the last job whose first block is <= b
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (pref[mid] <= b)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    const PrepJob& j = pp.jobs[lo];
+    const int local = b - pref[lo];
+    if (is_a) {
+        const int64_t total = (int64_t)j.m * (j.kp / 8);
+        const int64_t i = (int64_t)local * 256 + threadIdx.x;
+        if (i < total) split_a_chunk<PATH>(j.A, j.m, j.k, j.lda, j.kp, j.wa, i);
+    } else {
+        split_bt_tile<PATH>(j.B, j.k, j.n, j.ldb, j.kp, j.wb, local % j.b_tiles_n,
+                            local / j.b_tiles_n, tile);
+    }
+}
+
+// ------------------------------------------------- grouped split: host side --
+
+// Host copy of a grouped launch's tables, laid out as one blob so one copy
+// moves it to the device: problems | tiles | tensor maps (64-byte aligned) |
+// pre-pass jobs | A prefix sums | B prefix sums.
+struct GroupedTables {
+    std::vector<GSProblem> probs;
+    std::vector<GSTile> tiles;
+    std::vector<CUtensorMap> maps;
+    std::vector<PrepJob> jobs;
+    std::vector<int> a_prefix, b_prefix;
+    std::vector<int> k_zero;  // problems with k == 0 (plain path)
+    size_t off_tiles = 0, off_maps = 0, off_jobs = 0, off_apref = 0, off_bpref = 0, bytes = 0;
+};
+
+static size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+template <int PATH>
+static int grouped_tables(const sgemm_b200_problem* pr, void* const* ws, int count,
+                          GroupedTables* out) {
+    using T = Traits<PATH>;
+    GroupedTables gt;
+    gt.a_prefix.push_back(0);
+    gt.b_prefix.push_back(0);
+    for (int i = 0; i < count; ++i) {
+        const sgemm_b200_problem& q = pr[i];
+        if (q.m == 0 || q.n == 0) continue;
+        if (q.k == 0) {
+            gt.k_zero.push_back(i);
+            continue;
+        }
+        size_t a_bytes = 0;
+        workspace_bytes<PATH>(q.m, q.n, q.k, &a_bytes);
+        uint8_t* wa = reinterpret_cast<uint8_t*>(
+            (reinterpret_cast<uintptr_t>(ws[i]) + 1023) & ~static_cast<uintptr_t>(1023));
+        uint8_t* wb = wa + a_bytes;
+        const int kp = (q.k + 7) / 8 * 8;
+        const int idx = (int)gt.probs.size();
+        GSProblem g;
+        g.m = q.m;
+        g.n = q.n;
+        g.k = q.k;
+        g.ldc = q.ldc;
+        g.alpha = q.alpha;
+        g.beta = q.beta;
+        g.C = q.C;
+        g.vec_c = (q.ldc % 4 == 0) && (reinterpret_cast<uintptr_t>(q.C) % 16 == 0);
+        g.pad = 0;
+        gt.probs.push_back(g);
+        CUtensorMap ma, mb;
+        std::memset(&ma, 0, sizeof(ma));
+        std::memset(&mb, 0, sizeof(mb));
+        const CUtensorMapDataType dt =
+            T::ESZ == 2 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+        const uint64_t row = (uint64_t)kp * T::ESZ;
+        if (!encode_tensor_map_3d(&ma, dt, wa, (uint64_t)q.k, (uint64_t)q.m, T::NSPLIT, row,
+                                  row * (uint64_t)q.m, T::BK, BM, T::NSPLIT,
+                                  CU_TENSOR_MAP_SWIZZLE_64B) ||
+            !encode_tensor_map_3d(&mb, dt, wb, (uint64_t)q.k, (uint64_t)q.n, T::NSPLIT, row,
+                                  row * (uint64_t)q.n, T::BK, BN, T::NSPLIT,
+                                  CU_TENSOR_MAP_SWIZZLE_64B))
+            return SGEMM_B200_ERR_CUDA;
+        gt.maps.push_back(ma);
+        gt.maps.push_back(mb);
+        PrepJob j;
+        j.A = q.A;
+        j.B = q.B;
+        j.wa = wa;
+        j.wb = wb;
+        j.m = q.m;
+        j.n = q.n;
+        j.k = q.k;
+        j.kp = kp;
+        j.lda = q.lda;
+        j.ldb = q.ldb;
+        j.b_tiles_n = div_up(q.n, 64);
+        j.pad = 0;
+        gt.jobs.push_back(j);
+        const int64_t a_chunks = (int64_t)q.m * (kp / 8);
+        gt.a_prefix.push_back(gt.a_prefix.back() + (int)((a_chunks + 255) / 256));
+        gt.b_prefix.push_back(gt.b_prefix.back() + j.b_tiles_n * div_up(kp, 64));
+        const int nk = div_up(q.k, T::BK);
+        for (int a = 0; a < div_up(q.m, BM); ++a)
+            for (int b = 0; b < div_up(q.n, BN); ++b) gt.tiles.push_back(GSTile{idx, a, b, nk});
+    }
+    // longest first (all tiles have the same area; their cost is their k depth)
+    std::stable_sort(gt.tiles.begin(), gt.tiles.end(),
+                     [](const GSTile& x, const GSTile& y) { return x.nk > y.nk; });
+    gt.off_tiles = align_up(sizeof(GSProblem) * gt.probs.size(), 64);
+    gt.off_maps = align_up(gt.off_tiles + sizeof(GSTile) * gt.tiles.size(), 64);
+    gt.off_jobs = align_up(gt.off_maps + sizeof(CUtensorMap) * gt.maps.size(), 64);
+    gt.off_apref = align_up(gt.off_jobs + sizeof(PrepJob) * gt.jobs.size(), 64);
+    gt.off_bpref = align_up(gt.off_apref + sizeof(int) * gt.a_prefix.size(), 64);
+    gt.bytes = align_up(gt.off_bpref + sizeof(int) * gt.b_prefix.size(), 64);
+    *out = std::move(gt);
+    return SGEMM_B200_OK;
+}
+
+static void pack_tables(const GroupedTables& gt, uint8_t* h) {
+    std::memcpy(h, gt.probs.data(), sizeof(GSProblem) * gt.probs.size());
+    std::memcpy(h + gt.off_tiles, gt.tiles.data(), sizeof(GSTile) * gt.tiles.size());
+    std::memcpy(h + gt.off_maps, gt.maps.data(), sizeof(CUtensorMap) * gt.maps.size());
+    std::memcpy(h + gt.off_jobs, gt.jobs.data(), sizeof(PrepJob) * gt.jobs.size());
+    std::memcpy(h + gt.off_apref, gt.a_prefix.data(), sizeof(int) * gt.a_prefix.size());
+    std::memcpy(h + gt.off_bpref, gt.b_prefix.data(), sizeof(int) * gt.b_prefix.size());
+}
+
+// The grouped kernel's shared-memory attribute, once per device.
+template <int PATH>
+static int set_grouped_attribute() {
+    static std::atomic<bool> done[64];
+    static std::mutex mu;
+    const int dev = device_info().device;
+    if (dev < 0 || dev >= 64) return SGEMM_B200_ERR_CUDA;
+    if (done[dev].load(std::memory_order_acquire)) return SGEMM_B200_OK;
+    std::lock_guard<std::mutex> lock(mu);
+    if (!done[dev].load(std::memory_order_relaxed)) {
+        const cudaError_t e =
+            cudaFuncSetAttribute(split_grouped_kernel<PATH>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 Layout<PATH>::SMEM_BYTES);
+        if (e != cudaSuccess) return cuda_status(e);
+        done[dev].store(true, std::memory_order_release);
+    }
+    return SGEMM_B200_OK;
+}
+
+// Pre-pass and persistent kernel over the tables at device address d.
+template <int PATH>
+static int grouped_enqueue(const GroupedTables& gt, const uint8_t* d, cudaStream_t stream) {
+    if (gt.tiles.empty()) return SGEMM_B200_OK;
+    int st = set_grouped_attribute<PATH>();
+    if (st != SGEMM_B200_OK) return st;
+    PrepParams pp;
+    pp.jobs = reinterpret_cast<const PrepJob*>(d + gt.off_jobs);
+    pp.a_prefix = reinterpret_cast<const int*>(d + gt.off_apref);
+    pp.b_prefix = reinterpret_cast<const int*>(d + gt.off_bpref);
+    pp.n_jobs = (int)gt.jobs.size();
+    pp.a_blocks = gt.a_prefix.back();
+    const int blocks = gt.a_prefix.back() + gt.b_prefix.back();
+    split_prepass_grouped_kernel<PATH><<<blocks, 256, 0, stream>>>(pp);
+    GSParams gp;
+    gp.probs = reinterpret_cast<const GSProblem*>(d);
+    gp.tiles = reinterpret_cast<const GSTile*>(d + gt.off_tiles);
+    gp.maps = reinterpret_cast<const CUtensorMap*>(d + gt.off_maps);
+    gp.status = device_status_ptr();
+    gp.n_tiles = (int)gt.tiles.size();
+    if (!gp.status) return SGEMM_B200_ERR_CUDA;
+    const int sms = device_info().sm_count > 0 ? device_info().sm_count : 148;
+    const int grid = std::min(gp.n_tiles, sms);
+    split_grouped_kernel<PATH><<<grid, THREADS, Layout<PATH>::SMEM_BYTES, stream>>>(gp);
+    return cuda_status(cudaGetLastError());
+}
+
+template <int PATH>
+static int grouped_arena_launch(Arena* a, const sgemm_b200_problem* probs, void* const* ws,
+                                int count, cudaStream_t stream) {
+    GroupedTables gt;
+    int st = grouped_tables<PATH>(probs, ws, count, &gt);
+    if (st != SGEMM_B200_OK) return st;
+    if (!gt.tiles.empty()) {
+        if (gt.bytes > a->cap) {
+            // grow: generous first size (64 KiB covers ~100 problems), doubling
+            const size_t n = std::max({gt.bytes, a->cap * 2, (size_t)65536});
+            if (a->d) cudaFreeAsync(a->d, stream);
+            if (a->h) cudaFreeHost(a->h);
+            a->d = nullptr;
+            a->h = nullptr;
+            a->cap = 0;
+            cudaMemPool_t pool = library_pool();
+            if (!pool) return SGEMM_B200_ERR_CUDA;
+            cudaError_t e = cudaMallocFromPoolAsync(reinterpret_cast<void**>(&a->d), n, pool,
+                                                    stream);
+            if (e == cudaSuccess) e = cudaMallocHost(reinterpret_cast<void**>(&a->h), n);
+            if (e != cudaSuccess) return cuda_status(e);
+            a->cap = n;
+        }
+        pack_tables(gt, a->h);
+        st = cuda_status(cudaMemcpyAsync(a->d, a->h, gt.bytes, cudaMemcpyHostToDevice, stream));
+        if (st == SGEMM_B200_OK) st = grouped_enqueue<PATH>(gt, a->d, stream);
+        if (st != SGEMM_B200_OK) return st;
+    }
+    for (int i : gt.k_zero) {  // C := beta * C
+        const sgemm_b200_problem& q = probs[i];
+        st = plain_launch(-1, q.m, q.n, 0, q.alpha, q.A, q.lda, q.B, q.ldb, q.beta, q.C, q.ldc,
+                          stream);
+        if (st != SGEMM_B200_OK) return st;
+    }
+    return SGEMM_B200_OK;
+}
+
+size_t problem_workspace_bytes(int path, int m, int n, int k) {
+    if (m <= 0 || n <= 0 || k <= 0) return 0;
+    return path == SGEMM_B200_PATH_BF16X6 ? workspace_bytes<SGEMM_B200_PATH_BF16X6>(m, n, k)
+                                          : workspace_bytes<SGEMM_B200_PATH_TF32X3>(m, n, k);
+}
+
+int grouped_launch(Arena* a, int path, const sgemm_b200_problem* probs, void* const* ws,
+                   int count, cudaStream_t stream) {
+    if (!device_is_sm100()) return SGEMM_B200_ERR_UNSUPPORTED;
+    if (path == SGEMM_B200_PATH_BF16X6)
+        return grouped_arena_launch<SGEMM_B200_PATH_BF16X6>(a, probs, ws, count, stream);
+    if (path == SGEMM_B200_PATH_TF32X3)
+        return grouped_arena_launch<SGEMM_B200_PATH_TF32X3>(a, probs, ws, count, stream);
+    return SGEMM_B200_ERR_INVALID_ARG;
+}
+
+void arena_release(Arena* a) {
+    cudaFree(a->d);
+    cudaFreeHost(a->h);
+    *a = Arena();
+}
+
 }  // namespace split
 
 int split_launch(int path, int m, int n, int k, float alpha, const float* A, int lda,
@@ -579,6 +1159,90 @@ extern "C" int sgemm_b200_split(int path, int m, int n, int k, const float* alph
                               workspace_bytes, sgb::as_stream(stream));
     sgb::set_last_status(s);
     return s;
+}
+
+namespace sgb {
+namespace split {
+
+// One grouped launch with its workspace and tables allocated stream-ordered
+// from the library pool and freed after the kernels (the table upload is a
+// pageable copy, staged by the driver before the call returns).
+template <int PATH>
+static int grouped_oneshot(const sgemm_b200_problem* probs, int count, cudaStream_t stream) {
+    cudaMemPool_t pool = library_pool();
+    if (!pool) return SGEMM_B200_ERR_CUDA;
+    std::vector<size_t> off(count, 0);
+    size_t total = 0;
+    for (int i = 0; i < count; ++i) {
+        off[i] = total;
+        total += align_up(problem_workspace_bytes(PATH, probs[i].m, probs[i].n, probs[i].k), 1024);
+    }
+    uint8_t* ws = nullptr;
+    if (total) {
+        const cudaError_t e = cudaMallocFromPoolAsync(reinterpret_cast<void**>(&ws), total, pool,
+                                                      stream);
+        if (e != cudaSuccess) return cuda_status(e);
+    }
+    std::vector<void*> wsp(count);
+    for (int i = 0; i < count; ++i) wsp[i] = ws + off[i];
+    GroupedTables gt;
+    int st = grouped_tables<PATH>(probs, wsp.data(), count, &gt);
+    uint8_t* d = nullptr;
+    if (st == SGEMM_B200_OK && !gt.tiles.empty()) {
+        std::vector<uint8_t> h(gt.bytes);
+        pack_tables(gt, h.data());
+        st = cuda_status(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&d), gt.bytes, pool,
+                                                 stream));
+        if (st == SGEMM_B200_OK)
+            st = cuda_status(cudaMemcpyAsync(d, h.data(), gt.bytes, cudaMemcpyHostToDevice,
+                                             stream));
+        if (st == SGEMM_B200_OK) st = grouped_enqueue<PATH>(gt, d, stream);
+    }
+    for (size_t z = 0; st == SGEMM_B200_OK && z < gt.k_zero.size(); ++z) {
+        const sgemm_b200_problem& q = probs[gt.k_zero[z]];
+        st = plain_launch(-1, q.m, q.n, 0, q.alpha, q.A, q.lda, q.B, q.ldb, q.beta, q.C, q.ldc,
+                          stream);
+    }
+    if (d) cudaFreeAsync(d, stream);
+    if (ws) cudaFreeAsync(ws, stream);
+    return st;
+}
+
+}  // namespace split
+}  // namespace sgb
+
+extern "C" int sgemm_b200_grouped_split(int path, const sgemm_b200_problem* problems, int count,
+                                        sgemm_b200_stream_t stream) {
+    int s = SGEMM_B200_OK;
+    if (count < 0 || (count > 0 && !problems) ||
+        (path != SGEMM_B200_PATH_BF16X6 && path != SGEMM_B200_PATH_TF32X3))
+        s = SGEMM_B200_ERR_INVALID_ARG;
+    for (int i = 0; s == SGEMM_B200_OK && i < count; ++i) {
+        const sgemm_b200_problem& q = problems[i];
+        s = sgb::check_gemm_args(q.m, q.n, q.k, &q.alpha, q.A, q.lda, q.B, q.ldb, &q.beta, q.C,
+                                 q.ldc);
+    }
+    if (s == SGEMM_B200_OK && count > 0 && !sgb::device_is_sm100()) s = SGEMM_B200_ERR_UNSUPPORTED;
+    if (s == SGEMM_B200_OK && count > 0)
+        s = path == SGEMM_B200_PATH_BF16X6
+                ? sgb::split::grouped_oneshot<SGEMM_B200_PATH_BF16X6>(problems, count,
+                                                                      sgb::as_stream(stream))
+                : sgb::split::grouped_oneshot<SGEMM_B200_PATH_TF32X3>(problems, count,
+                                                                      sgb::as_stream(stream));
+    sgb::set_last_status(s);
+    return s;
+}
+
+extern "C" int sgemm_b200_grouped_split_sequential(int path, const sgemm_b200_problem* problems,
+                                                   int count, sgemm_b200_stream_t stream) {
+    if (count < 0 || (count > 0 && !problems)) return SGEMM_B200_ERR_INVALID_ARG;
+    for (int i = 0; i < count; ++i) {
+        const sgemm_b200_problem& q = problems[i];
+        const int s = sgemm_b200_split(path, q.m, q.n, q.k, &q.alpha, q.A, q.lda, q.B, q.ldb,
+                                       &q.beta, q.C, q.ldc, nullptr, 0, stream);
+        if (s != SGEMM_B200_OK) return s;
+    }
+    return SGEMM_B200_OK;
 }
 
 extern "C" int sgemm_b200_gemm(int path, int m, int n, int k, const float* alpha, const float* A,

@@ -140,6 +140,8 @@ def _declare(lib: ctypes.CDLL) -> None:
       [ctypes.POINTER(Problem), _I, ctypes.c_char_p, ctypes.POINTER(_I), ctypes.POINTER(_I),
        ctypes.POINTER(ctypes.c_size_t)])
     d("sgemm_b200_grouped_bucket", _I, [_I, _I, _I])
+    d("sgemm_b200_grouped_split", _I, [_I, ctypes.POINTER(Problem), _I, _P])
+    d("sgemm_b200_grouped_split_sequential", _I, [_I, ctypes.POINTER(Problem), _I, _P])
     d("sgemm_b200_autotune_grouped", _I, [ctypes.POINTER(Problem), _I, ctypes.c_char_p])
     d("sgemm_b200_fill_random", _I, [_P, _I, _I, _I, ctypes.c_uint64, ctypes.c_uint32, _I, _P])
     d("sgemm_b200_device_status", _I, [])
@@ -156,6 +158,13 @@ def _declare(lib: ctypes.CDLL) -> None:
     d("sgemm_b200_server_destroy", None, [_P])
     d("sgemm_b200_server_submit", _I, [_P, _I, _I, _I, ctypes.c_float, ctypes.c_float,
                                       ctypes.c_uint64, ctypes.POINTER(ctypes.c_int64)])
+    d("sgemm_b200_server_submit_device", _I, [_P, _I, _I, _I, ctypes.c_float, _P, _I, _P, _I,
+                                             ctypes.c_float, _P, _I,
+                                             ctypes.POINTER(ctypes.c_int64)])
+    d("sgemm_b200_server_submit_host", _I, [_P, _I, _I, _I, ctypes.c_float, _P, _I, _P, _I,
+                                           ctypes.c_float, _P, _I, ctypes.POINTER(ctypes.c_int64)])
+    d("sgemm_b200_server_wait", _I, [_P, ctypes.c_int64, ctypes.POINTER(ctypes.c_double)])
+    d("sgemm_b200_server_isolated_ms", _I, [_P, _I, _I, _I, _I, ctypes.POINTER(ctypes.c_double)])
     d("sgemm_b200_server_drain", _I, [_P])
     d("sgemm_b200_server_result", _I, [_P, ctypes.c_int64, ctypes.POINTER(ctypes.c_double),
                                       ctypes.POINTER(_P), ctypes.POINTER(_I), ctypes.POINTER(_I)])
@@ -382,6 +391,22 @@ def grouped_sequential(problems, stream=None) -> None:
            "grouped_sequential")
 
 
+def grouped_split(path, problems, stream=None) -> None:
+    """All problems through one grouped split pre-pass and one persistent
+    tcgen05 launch (path 'bf16x6' or 'tf32x3')."""
+    p = PATHS[path] if isinstance(path, str) else int(path)
+    _check(lib().sgemm_b200_grouped_split(p, problems, len(problems), _stream_ptr(stream)),
+           "grouped_split")
+
+
+def grouped_split_sequential(path, problems, stream=None) -> None:
+    """The baseline: one sgemm_b200_split call per problem, in order."""
+    p = PATHS[path] if isinstance(path, str) else int(path)
+    _check(lib().sgemm_b200_grouped_split_sequential(p, problems, len(problems),
+                                                     _stream_ptr(stream)),
+           "grouped_split_sequential")
+
+
 def grouped_schedule(problems, tuning_json: Optional[str] = None) -> dict:
     """Host-only schedule summary (tiles, work items, split-K workspace bytes)."""
     t, w, b = ctypes.c_int(), ctypes.c_int(), ctypes.c_size_t()
@@ -467,6 +492,52 @@ class Server:
         _check(lib().sgemm_b200_server_submit(self._h, m, n, k, alpha, beta, seed,
                                               ctypes.byref(rid)), "server_submit")
         return rid.value
+
+    def submit_device(self, A, B, C, alpha: float = 1.0, beta: float = 0.0) -> int:
+        """C := alpha*A@B + beta*C on the caller's CUDA tensors, in place on C.
+        The tensors must be ready on the device (synchronise their stream
+        first) and left untouched until the request completes."""
+        m, k = A.shape
+        n = B.shape[1]
+        if B.shape[0] != k or tuple(C.shape) != (m, n):
+            raise ValueError("shape mismatch")
+        pa, lda = _mat(A, "A")
+        pb, ldb = _mat(B, "B")
+        pc, ldc = _mat(C, "C")
+        rid = ctypes.c_int64()
+        _check(lib().sgemm_b200_server_submit_device(self._h, m, n, k, alpha, pa, lda, pb, ldb,
+                                                     beta, pc, ldc, ctypes.byref(rid)),
+               "server_submit_device")
+        return rid.value
+
+    def submit_host(self, A, B, C, alpha: float = 1.0, beta: float = 0.0) -> int:
+        """The same with host (CPU, ideally pinned) tensors: the server copies
+        them in at admission and C back after the batch."""
+        m, k = A.shape
+        n = B.shape[1]
+        if B.shape[0] != k or tuple(C.shape) != (m, n):
+            raise ValueError("shape mismatch")
+        pa, lda = _mat(A, "A", "cpu")
+        pb, ldb = _mat(B, "B", "cpu")
+        pc, ldc = _mat(C, "C", "cpu")
+        rid = ctypes.c_int64()
+        _check(lib().sgemm_b200_server_submit_host(self._h, m, n, k, alpha, pa, lda, pb, ldb,
+                                                   beta, pc, ldc, ctypes.byref(rid)),
+               "server_submit_host")
+        return rid.value
+
+    def wait(self, rid: int) -> float:
+        """Block until the request completes; returns its latency in ms."""
+        lat = ctypes.c_double()
+        _check(lib().sgemm_b200_server_wait(self._h, rid, ctypes.byref(lat)), "server_wait")
+        return lat.value
+
+    def isolated_ms(self, m: int, n: int, k: int, reps: int = 5) -> float:
+        """Device time of one m x n x k request served alone (server idle)."""
+        ms = ctypes.c_double()
+        _check(lib().sgemm_b200_server_isolated_ms(self._h, m, n, k, reps, ctypes.byref(ms)),
+               "server_isolated_ms")
+        return ms.value
 
     def drain(self) -> None:
         _check(lib().sgemm_b200_server_drain(self._h), "server_drain")
