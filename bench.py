@@ -571,6 +571,38 @@ def _grouped_leg(torch, sg, sms, sm_mhz, hbm_gbs, count=512):
     t_tuned = timed(lambda: plan.launch(use_graph=True), 7)
     tinfo = plan.info()
     plan.close()
+    # a workload where the tuner's choice matters: 32 problems of 256 x 256 x
+    # 32768 (256 tiles for 444 resident CTA slots, so split-K pays)
+    kspecs = []
+    for i in range(32):
+        A = torch.empty((256, 32768), device="cuda")
+        B = torch.empty((32768, 256), device="cuda")
+        C = torch.zeros((256, 256), device="cuda")
+        sg.fill_random(A, 1200 + i, 1, 0)
+        sg.fill_random(B, 1200 + i, 2, 0)
+        kspecs.append((A, B, C, 1.0, 0.0))
+    kprobs = sg.make_problems(kspecs)
+    ktuned = os.path.join("/tmp", f"sgemm_b200_grouped_ktuning_{os.getpid()}.json")
+    sg.autotune_grouped(kprobs, ktuned)
+    with open(ktuned) as f:
+        ktable = json.load(f)
+    plan = sg.GroupedPlan(kspecs)
+    tk_default = timed(lambda: plan.launch(use_graph=True), 7)
+    plan.close()
+    plan = sg.GroupedPlan(kspecs, tuning_json=ktuned)
+    tk_tuned = timed(lambda: plan.launch(use_graph=True), 7)
+    kinfo = plan.info()
+    plan.close()
+    os.unlink(ktuned)
+    kflop = 32 * 2.0 * 256 * 256 * 32768
+    k_heavy = {"workload": "32 problems of 256 x 256 x 32768, alpha=1 beta=0",
+               "default_ms": round(tk_default, 3), "tuned_ms": round(tk_tuned, 3),
+               "default_gflops": round(kflop / tk_default * 1e-6, 1),
+               "tuned_gflops": round(kflop / tk_tuned * 1e-6, 1),
+               "speedup": round(tk_default / tk_tuned, 3), "work_items_tuned": kinfo["work_items"],
+               "tuned_buckets": [b for b in ktable["buckets"] if b["split"] > 1 or
+                                 b["tile"] != 0 or b.get("stages", 4) != 4]}
+    del kspecs, kprobs
     # the same 512 problems on the split-precision path: one grouped pre-pass +
     # one persistent tcgen05 launch, against one sgemm_b200_split call each
     split = {}
@@ -610,6 +642,7 @@ def _grouped_leg(torch, sg, sms, sm_mhz, hbm_gbs, count=512):
         "launches": 1, "tiles": info["tiles"], "work_items_default": info["work_items"],
         "work_items_tuned": tinfo["work_items"], "autotune_s": round(tune_s, 1),
         "tuning": table,
+        "tuner_k_heavy": k_heavy,
         "split_paths": split,
     }
 

@@ -30,6 +30,15 @@ using C9 = Cfg<128, 128, 4, 2, 8, 3, kLoaderAsync4, 2>;
 using C11 = Cfg<64, 128, 2, 2, 8, 4, kLoaderAsync4, 2>;
 using C12 = Cfg<64, 64, 2, 1, 8, 4, kLoaderAsync4, 3>;
 using C14 = Cfg<128, 64, 4, 1, 8, 3, kLoaderAsync4, 3>;
+// The 128 x 64 tile with twice the warps (8 x 4 threads): for problems that
+// are a single partial wave, where each busy SM holds one tile and four warps
+// cannot hide the shared-memory and barrier latency.
+using W0 = Cfg<128, 64, 4, 2, 4, 3, kLoaderTma, 3>;        // 8 warps,  72 KB
+using W1 = Cfg<128, 64, 4, 2, 4, 4, kLoaderTma, 2>;        // 8 warps,  96 KB
+// The best large tile with a producer warp (per-stage empty mbarriers, no CTA
+// barrier in the main loop).
+using P0 = Cfg<128, 64, 4, 1, 8, 3, kLoaderTma, 3, 8, 1>;  // 4+1 warps, 72 KB
+using P1 = Cfg<128, 64, 4, 1, 8, 4, kLoaderTma, 2, 8, 1>;  // 4+1 warps, 96 KB
 
 struct ConfigDesc {
     const char* name;
@@ -61,6 +70,8 @@ static const ConfigDesc kConfigs[] = {
     describe<S1>("tma_32x64_w2_t8x4_s4", 0.700f),      describe<C8>("cpa_128x256_w8_t8x16_s4", 1.000f),
     describe<C9>("cpa_128x128_w8_t8x8_s3", 0.920f),    describe<C11>("cpa_64x128_w4_t8x8_s4", 0.810f),
     describe<C12>("cpa_64x64_w2_t8x8_s4", 0.630f),     describe<C14>("cpa_128x64_w4_t8x8_s3", 0.890f),
+    describe<W0>("tma_128x64_w8_t8x4_s3", 0.700f),     describe<W1>("tma_128x64_w8_t8x4_s4", 0.700f),
+    describe<P0>("tma_128x64_w4p_t8x8_s3", 0.700f),    describe<P1>("tma_128x64_w4p_t8x8_s4", 0.700f),
 };
 constexpr int kNumConfigs = sizeof(kConfigs) / sizeof(kConfigs[0]);
 

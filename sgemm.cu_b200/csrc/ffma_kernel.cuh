@@ -37,15 +37,20 @@ namespace ffma {
 enum Loader { kLoaderTma = 0, kLoaderAsync4 = 1 };
 
 template <int BM_, int BN_, int WM_, int WN_, int TN_, int STAGES_, int LOADER_, int MINB_ = 1,
-          int K4U_ = 8>
+          int K4U_ = 8, int PRODUCER_ = 0>
 struct Cfg {
     static constexpr int BM = BM_, BN = BN_, WM = WM_, WN = WN_, TN = TN_, STAGES = STAGES_;
     static constexpr int LOADER = LOADER_;
     static constexpr int MINB = MINB_;  // resident CTAs per SM the register budget targets
     static constexpr int K4U = K4U_;    // unroll of the 8 four-deep k steps of a k block
+    // PRODUCER: one extra warp issues the TMA loads, and the compute warps free
+    // each stage through a per-stage "empty" mbarrier instead of a CTA barrier.
+    static constexpr int PRODUCER = PRODUCER_;
     static constexpr int BK = 32;  // one 128-byte row of A per k block
     static constexpr int TM = 8;
-    static constexpr int THREADS = 32 * WM * WN;
+    static constexpr int COMPUTE_THREADS = 32 * WM * WN;
+    static constexpr int THREADS = COMPUTE_THREADS + (PRODUCER ? 32 : 0);
+    static_assert(!PRODUCER || LOADER_ == 0, "the producer warp issues TMA loads");
     static_assert(BM == WM * 4 * TM, "4 lanes x 8 rows per warp along m");
     static_assert(BN == WN * 8 * TN, "8 lanes x TN columns per warp along n");
     static_assert(TN % 4 == 0, "columns come in float4 groups");
@@ -254,10 +259,77 @@ __global__ void __launch_bounds__(C::THREADS, C::MINB)
                      const __grid_constant__ CUtensorMap tmB, const Params p) {
     extern __shared__ uint8_t smem_raw[];
     __shared__ __align__(8) uint64_t full_bar[C::STAGES];
+    __shared__ __align__(8) uint64_t empty_bar[C::PRODUCER ? C::STAGES : 1];
     uint8_t* smem = align_smem_1024(smem_raw);
 
     const int tid = threadIdx.x;
     const int warp = tid >> 5, lane = tid & 31;
+
+    if constexpr (C::PRODUCER) {
+        int tm, tn;
+        tile_coords(blockIdx.x, p.tiles_m, p.tiles_n, tm, tn);
+        const int nk = (p.op.k + C::BK - 1) / C::BK;
+        if (tid == 0) {
+            for (int s = 0; s < C::STAGES; ++s) {
+                mbar_init(&full_bar[s], 1);
+                mbar_init(&empty_bar[s], C::WM * C::WN);  // one arrival per compute warp
+            }
+            fence_barrier_init();
+        }
+        __syncthreads();  // the only CTA-wide barrier: barriers initialised
+        if (warp == C::WM * C::WN) {
+            // ------------------------------------------------ TMA producer --
+            if (lane == 0 && nk > 0) {
+                tma_prefetch_desc(&tmA);
+                tma_prefetch_desc(&tmB);
+                int kb = 0;
+                for (; kb < nk; ++kb) {
+                    const int s = kb % C::STAGES;
+                    if (kb >= C::STAGES &&
+                        !mbar_wait(&empty_bar[s], ((kb / C::STAGES) - 1) & 1)) {
+                        atomicExch(p.status, SGEMM_B200_ERR_TIMEOUT);
+                        break;
+                    }
+                    uint8_t* st = smem + s * C::STAGE_BYTES;
+                    mbar_arrive_expect_tx(&full_bar[s], C::STAGE_BYTES);
+                    tma_load_2d(st, &tmA, &full_bar[s], kb * C::BK, tm * C::BM);
+                    tma_load_2d(st + C::A_BYTES, &tmB, &full_bar[s], tn * C::BN, kb * C::BK);
+                }
+                // Copies still in flight land before the CTA's smem is released
+                // (the compute warps may have given up on a stage).
+                for (int j = (kb > C::STAGES ? kb - C::STAGES : 0); j < kb; ++j)
+                    if (!mbar_wait(&full_bar[j % C::STAGES], (j / C::STAGES) & 1)) break;
+            }
+            return;
+        }
+        const int wm = warp / C::WN, wn = warp % C::WN;
+        int lm, ln;
+        lane_coords(lane, lm, ln);
+        const int m0 = tm * C::BM, n0 = tn * C::BN;
+        const uint32_t a_base = static_cast<uint32_t>((wm * 32 + lm) * 128);
+        const uint32_t xa0 = static_cast<uint32_t>(lm) << 4;
+        const uint32_t xa1 = static_cast<uint32_t>(lm + 4) << 4;
+        const uint32_t b_base = static_cast<uint32_t>((wn * 8 * C::TN + ln * 4) * 4);
+        float acc[C::TM][C::TN];
+#pragma unroll
+        for (int i = 0; i < C::TM; ++i)
+#pragma unroll
+            for (int j = 0; j < C::TN; ++j) acc[i][j] = 0.0f;
+        for (int kb = 0; kb < nk; ++kb) {
+            const int s = kb % C::STAGES;
+            if (!mbar_wait(&full_bar[s], (kb / C::STAGES) & 1)) {
+                if (lane == 0) atomicExch(p.status, SGEMM_B200_ERR_TIMEOUT);
+                return;
+            }
+            const uint8_t* st = smem + s * C::STAGE_BYTES;
+            compute_stage<C>(st, st + C::A_BYTES, a_base, xa0, xa1, b_base, acc);
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&empty_bar[s]);  // this warp is done with the stage
+        }
+        epilogue<C>(p.op, m0, n0, wm, wn, lm, ln, acc);
+        return;
+    }
+
     const int wm = warp / C::WN, wn = warp % C::WN;
     int lm, ln;
     lane_coords(lane, lm, ln);

@@ -80,6 +80,7 @@ struct GProblem {
     int tma;       // tensor maps valid
     int split;     // k splits
     int kbps;      // k blocks per split
+    int depth;     // k blocks kept in flight through the stage ring (2..S)
     int tiles_n;
     int cnt_base;  // first tile ticket (split > 1)
     long long ws_base;  // first workspace float (split > 1)
@@ -145,7 +146,8 @@ __device__ __forceinline__ bool run_item(const GParams& gp, const GProblem& pr, 
             tma_load_2d(st + C::A_BYTES, tmB, &full_bar[s], n0, (kb0 + j) * C::BK);
         };
         if (tid == 0) {
-            for (; issued < S && issued < nkb; ++issued) issue(issued);
+            const int depth = min(S, pr.depth);  // the bucket's stage count
+            for (; issued < depth && issued < nkb; ++issued) issue(issued);
         }
         for (int j = 0; j < nkb; ++j) {
             const uint32_t gs = g + j;
@@ -289,6 +291,7 @@ __global__ void __launch_bounds__(THREADS, (S == 3 ? 3 : 2)) grouped_kernel(cons
 struct Choice {
     int tile = kTileTall;
     int split = 1;
+    int depth = 4;  // stage count: k blocks in flight (capped by the launch's ring)
 };
 
 // Size buckets: M*N class x K class.
@@ -300,17 +303,12 @@ inline int bucket_of(int m, int n, int k) {
     return a * kKClasses + b;
 }
 
+// The tuning table: the launch's ring size (3 stages and 3 CTAs per SM, or 4
+// and 2) and, per size bucket, tile shape, split-K and stage count (how many
+// of the ring's stages a problem's items keep in flight).
 struct Table {
-    int stages = 3;  // 3 CTAs per SM; the autotuner may pick 4 (2 per SM)
+    int stages = 3;
     Choice c[kBuckets];
-    Table() {
-        for (int a = 0; a < kMnClasses; ++a)
-            for (int b = 0; b < kKClasses; ++b) {
-                Choice& ch = c[a * kKClasses + b];
-                ch.tile = kTileTall;
-                ch.split = 1;
-            }
-    }
 };
 
 static bool load_table(const char* path, Table* t) {
@@ -330,17 +328,21 @@ static bool load_table(const char* path, Table* t) {
         }
         if (line.find("\"sm_count\"") != std::string::npos)
             std::sscanf(line.c_str() + line.find(':') + 1, "%d", &sms);
-        if (line.find("\"stages\"") != std::string::npos)
+        // the launch's ring size (bucket lines carry their own "stages")
+        if (line.find("\"stages\"") != std::string::npos &&
+            line.find("{\"mn\"") == std::string::npos)
             std::sscanf(line.c_str() + line.find(':') + 1, "%d", &stages);
-        int mn, kc, tile, split;
+        int mn, kc, tile, split, depth = 4;
         const size_t p = line.find("{\"mn\"");
         if (p != std::string::npos &&
-            std::sscanf(line.c_str() + p, "{\"mn\": %d, \"k\": %d, \"tile\": %d, \"split\": %d", &mn,
-                        &kc, &tile, &split) == 4 &&
-            mn >= 0 && mn < kMnClasses && kc >= 0 && kc < kKClasses && (tile == 0 || tile == 1) &&
-            split >= 1 && split <= 16) {
+            std::sscanf(line.c_str() + p,
+                        "{\"mn\": %d, \"k\": %d, \"tile\": %d, \"split\": %d, \"stages\": %d", &mn,
+                        &kc, &tile, &split, &depth) >= 4 &&
+            mn >= 0 && mn < kMnClasses && kc >= 0 && kc < kKClasses && tile >= 0 && tile <= 2 &&
+            split >= 1 && split <= 16 && depth >= 2 && depth <= 4) {
             out.c[mn * kKClasses + kc].tile = tile;
             out.c[mn * kKClasses + kc].split = split;
+            out.c[mn * kKClasses + kc].depth = depth;
             ++seen;
         }
     }
@@ -356,7 +358,7 @@ static bool save_table(const char* path, const Table& t) {
     std::ofstream f(path);
     if (!f) return false;
     const DeviceInfo& di = device_info();
-    f << "{\n \"format\": \"sgemm_b200 grouped tuning v1\",\n";
+    f << "{\n \"format\": \"sgemm_b200 grouped tuning v2\",\n";
     f << " \"device\": \"" << di.name << "\",\n";
     f << " \"sm_count\": " << di.sm_count << ",\n";
     f << " \"stages\": " << t.stages << ",\n";
@@ -365,7 +367,7 @@ static bool save_table(const char* path, const Table& t) {
         for (int b = 0; b < kKClasses; ++b) {
             const Choice& ch = t.c[a * kKClasses + b];
             f << "  {\"mn\": " << a << ", \"k\": " << b << ", \"tile\": " << ch.tile
-              << ", \"split\": " << ch.split << "}"
+              << ", \"split\": " << ch.split << ", \"stages\": " << ch.depth << "}"
               << (a == kMnClasses - 1 && b == kKClasses - 1 ? "\n" : ",\n");
         }
     f << " ]\n}\n";
@@ -477,6 +479,7 @@ static int make_schedule(const sgemm_b200_problem* probs, int count, const Table
         g.kbps = nk > 0 ? div_up(nk, split) : 0;
         if (g.kbps > 0) split = div_up(nk, g.kbps);  // no empty splits
         g.split = split;
+        g.depth = ch.depth;
         const int tm = q.m > 0 ? div_up(q.m, bm) : 0;
         const int tn = q.n > 0 ? div_up(q.n, bn) : 0;
         g.tiles_n = tn;
@@ -866,8 +869,9 @@ extern "C" int sgemm_b200_autotune_grouped(const sgemm_b200_problem* problems, i
         return ms;
     };
     double best_ms = measure(best);
-    // Stage count (one per launch), then tile shape and split-K per bucket by
-    // coordinate descent over the buckets present in the workload.
+    // The launch's ring size, then per bucket present in the workload (by
+    // coordinate descent): tile shape x split-K, then the bucket's stage count.
+    // A candidate must win by 1% to replace the current choice.
     for (int st : {3, 4}) {
         if (st == best.stages) continue;
         Table t = best;
@@ -878,22 +882,33 @@ extern "C" int sgemm_b200_autotune_grouped(const sgemm_b200_problem* problems, i
             best = t;
         }
     }
+    auto consider = [&](const Table& t) {
+        const double ms = measure(t);
+        if (ms < best_ms * 0.99) {
+            best_ms = ms;
+            best = t;
+        }
+    };
     for (int b = 0; b < kBuckets; ++b) {
         if (!present[b]) continue;
-        const int kclass = b % kKClasses;
-        for (int tile : {kTileTall, kTileWide})
-            for (int split : {1, 2, 4, 8}) {
-                if (split > 1 && kclass == 0) continue;
+        const int kclass = b % kKClasses, mnclass = b / kKClasses;
+        for (int tile : {kTileTall, kTileWide, kTileSkinny}) {
+            if (tile == kTileSkinny && mnclass == 2) continue;  // large problems: no
+            for (int split : {1, 2, 4, 8, 16}) {
+                if (split > 1 && kclass == 0) continue;  // short K: nothing to split
                 Table t = best;
                 t.c[b].tile = tile;
                 t.c[b].split = split;
                 if (t.c[b].tile == best.c[b].tile && t.c[b].split == best.c[b].split) continue;
-                const double ms = measure(t);
-                if (ms < best_ms * 0.99) {
-                    best_ms = ms;
-                    best = t;
-                }
+                consider(t);
             }
+        }
+        for (int depth : {2, 3, 4}) {
+            if (depth == best.c[b].depth) continue;
+            Table t = best;
+            t.c[b].depth = depth;
+            consider(t);
+        }
     }
     cudaStreamDestroy(s);
     return save_table(json_path, best) ? SGEMM_B200_OK : SGEMM_B200_ERR_INVALID_ARG;

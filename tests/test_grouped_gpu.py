@@ -17,10 +17,13 @@ def _torch():
     return torch
 
 
-def _table(path, split, tile=1, stages=3):
+def _table(path, split, tile=1, stages=3, depth=None):
     torch = _torch()
     p = torch.cuda.get_device_properties(0)
     buckets = [{"mn": a, "k": b, "tile": tile, "split": split} for a in range(3) for b in range(3)]
+    if depth is not None:  # the buckets' own stage count
+        for x in buckets:
+            x["stages"] = depth
     lines = ",\n".join("  " + json.dumps(x) for x in buckets)
     path.write_text(f'{{\n "device": "{p.name}",\n "sm_count": {p.multi_processor_count},\n'
                     f' "stages": {stages},\n "buckets": [\n{lines}\n ]\n}}\n')
@@ -237,3 +240,65 @@ def test_autotuner_writes_table_and_plan_uses_it(tmp_path):
         want = A.double() @ B.double()
         assert torch.allclose(C.double(), want, rtol=0, atol=1e-5 * want.abs().max().item())
     plan.close()
+
+
+@pytest.mark.parametrize("depth", [2, 3])
+def test_bucket_stage_count_keeps_results(tmp_path, depth):
+    """A bucket's stage count changes only how many k blocks each item keeps
+    in flight through the ring, never the arithmetic: results stay equal to
+    the plain path's, bit for bit (4-stage ring, split 1)."""
+    torch = _torch()
+    specs, host = _make(SHAPES, 300, _lds())
+    plan = sg.GroupedPlan(specs, tuning_json=_table(tmp_path / "t.json", 1, tile=0, stages=4,
+                                                    depth=depth))
+    plan.launch(use_graph=True)
+    torch.cuda.synchronize()
+    assert sg.device_status() == sg.OK
+    for (dA, dB, dC, a, b), (A, B, C, _, _) in zip(specs, host):
+        assert np.array_equal(dC.cpu().numpy(), oracle.sgemm_basic(A, B, C, a, b, basic=False))
+    plan.close()
+
+
+def test_autotuner_beats_default_on_k_heavy_problems(tmp_path):
+    """32 problems of 256 x 256 x 32768: 256 tiles leave most of the GPU's
+    resident slots idle, so the default plan (no split-K) is far from the
+    tuned one, which splits K; the tuned plan is faster and its results stay
+    within FP32 accuracy (the split sums are reduced in a fixed order)."""
+    torch = _torch()
+    specs = []
+    for i in range(32):
+        A = torch.empty((256, 32768), device="cuda")
+        B = torch.empty((32768, 256), device="cuda")
+        C = torch.zeros((256, 256), device="cuda")
+        sg.fill_random(A, 1200 + i, 1, 0)
+        sg.fill_random(B, 1200 + i, 2, 0)
+        specs.append((A, B, C, 1.0, 0.0))
+    probs = sg.make_problems(specs)
+    path = str(tmp_path / "tuned.json")
+    sg.autotune_grouped(probs, path)
+    table = json.loads(open(path).read())
+    print(table)
+    assert any(b["split"] > 1 for b in table["buckets"])
+
+    def time_plan(plan):
+        plan.launch()
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(5):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            plan.launch()
+            b.record()
+            torch.cuda.synchronize()
+            ts.append(a.elapsed_time(b))
+        return sorted(ts)[2]
+
+    default, tuned = sg.GroupedPlan(specs), sg.GroupedPlan(specs, tuning_json=path)
+    t_default, t_tuned = time_plan(default), time_plan(tuned)
+    print(f"default {t_default:.3f} ms, tuned {t_tuned:.3f} ms")
+    assert t_tuned < 0.8 * t_default
+    for (A, B, C, a, b) in specs[:4]:
+        want = A.double() @ B.double()
+        assert torch.allclose(C.double(), want, rtol=0, atol=1e-5 * want.abs().max().item())
+    default.close()
+    tuned.close()
