@@ -247,6 +247,73 @@ __device__ __forceinline__ void epilogue(const Operands& p, int m0, int n0, int 
     }
 }
 
+// Epilogue for C rows that are not 16-byte aligned (ldc % 4 != 0 or an
+// unaligned base), where float4 accesses are impossible and per-thread
+// scalar accesses would touch 4 rows x 4 sectors per warp instruction for
+// 128 useful bytes.  Each warp first parks its 32 x (8 TN) outputs in shared
+// memory (the stage ring, free once the main loop is done), then walks its
+// rows with consecutive lanes on consecutive columns: one 128-byte row
+// segment per instruction.  The arithmetic per element is the epilogue's
+// (acc * alpha, then fma(C, beta, .)); only the thread that does it changes.
+// The caller must have made every warp finish reading the ring.
+template <class C>
+__device__ __forceinline__ void epilogue_staged(const Operands& p, int m0, int n0, int wm, int wn,
+                                                int lm, int ln, int warp, int lane,
+                                                const float (&acc)[C::TM][C::TN], uint8_t* smem) {
+    constexpr int W = 8 * C::TN;  // columns of a warp's tile
+    constexpr int LD = W + 8;     // row pitch: 8 banks between rows, conflict-free float4 stores
+    static_assert((C::COMPUTE_THREADS / 32) * 32 * LD * 4 <= C::STAGES * C::STAGE_BYTES,
+                  "the staged tile fits in the stage ring");
+    float* buf = reinterpret_cast<float*>(smem) + warp * 32 * LD;
+#pragma unroll
+    for (int i = 0; i < C::TM; ++i)
+#pragma unroll
+        for (int g = 0; g < C::TN / 4; ++g)
+            *reinterpret_cast<float4*>(buf + (lm + 4 * i) * LD + 4 * ln + 32 * g) =
+                make_float4(acc[i][4 * g], acc[i][4 * g + 1], acc[i][4 * g + 2], acc[i][4 * g + 3]);
+    __syncwarp();
+    const int col0 = n0 + wn * W;
+    for (int r = 0; r < 32; ++r) {
+        const int row = m0 + wm * 32 + r;
+        if (row >= p.m) break;
+        float* crow = p.C + (int64_t)row * p.ldc;
+#pragma unroll
+        for (int t = 0; t < W / 32; ++t) {
+            const int col = col0 + lane + 32 * t;
+            if (col < p.n) {
+                float v = __fmul_rn(buf[r * LD + lane + 32 * t], p.alpha);
+                if (p.beta != 0.0f) v = fmaf(crow[col], p.beta, v);
+                crow[col] = v;
+            }
+        }
+    }
+}
+
+// Barrier over the compute warps only (the producer warp, if any, has left).
+template <class C>
+__device__ __forceinline__ void compute_barrier() {
+    if constexpr (C::PRODUCER)
+        asm volatile("bar.sync 1, %0;" ::"n"(C::COMPUTE_THREADS) : "memory");
+    else
+        __syncthreads();
+}
+
+// The epilogue for any C: float4 stores straight from registers when C rows
+// are 16-byte aligned, else the shared-memory staged form.  Called by every
+// compute thread of the CTA (the staged form has a barrier).
+template <class C>
+__device__ __forceinline__ void epilogue_any(const Operands& p, int m0, int n0, int wm, int wn,
+                                             int lm, int ln, const float (&acc)[C::TM][C::TN],
+                                             uint8_t* smem) {
+    if (p.vec_c) {
+        epilogue<C>(p, m0, n0, wm, wn, lm, ln, acc);
+    } else {
+        compute_barrier<C>();  // every warp is done reading the stage ring
+        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+        epilogue_staged<C>(p, m0, n0, wm, wn, lm, ln, warp, lane, acc, smem);
+    }
+}
+
 struct Params {
     Operands op;  // vec_c: C rows are 16-byte aligned (ldc % 4 == 0 and C aligned)
     int* status;
@@ -326,7 +393,7 @@ __global__ void __launch_bounds__(C::THREADS, C::MINB)
             __syncwarp();
             if (lane == 0) mbar_arrive(&empty_bar[s]);  // this warp is done with the stage
         }
-        epilogue<C>(p.op, m0, n0, wm, wn, lm, ln, acc);
+        epilogue_any<C>(p.op, m0, n0, wm, wn, lm, ln, acc, smem);
         return;
     }
 
@@ -420,7 +487,7 @@ __global__ void __launch_bounds__(C::THREADS, C::MINB)
         cp_async_wait<0>();
     }
 
-    epilogue<C>(p.op, m0, n0, wm, wn, lm, ln, acc);
+    epilogue_any<C>(p.op, m0, n0, wm, wn, lm, ln, acc, smem);
 }
 
 }  // namespace ffma

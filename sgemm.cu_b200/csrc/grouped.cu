@@ -193,7 +193,7 @@ __device__ __forceinline__ bool run_item(const GParams& gp, const GProblem& pr, 
     }
 
     if (pr.split == 1) {
-        ffma::epilogue<C>(pr.op, m0, n0, wm, wn, lm, ln, acc);
+        ffma::epilogue_any<C>(pr.op, m0, n0, wm, wn, lm, ln, acc, smem);
         return true;
     }
 
@@ -241,7 +241,7 @@ __device__ __forceinline__ bool run_item(const GParams& gp, const GProblem& pr, 
                 }
         }
         (void)NQ;
-        ffma::epilogue<C>(pr.op, m0, n0, wm, wn, lm, ln, acc);
+        ffma::epilogue_any<C>(pr.op, m0, n0, wm, wn, lm, ln, acc, smem);
     }
     return true;
 }
