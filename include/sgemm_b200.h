@@ -120,6 +120,23 @@ int sgemm_b200_packs(int m, int n, int k,
                      const float* A, int lda,
                      const float* B, int ldb);
 
+/* Replaces the reference's pre-Ampere texture path (src/sgemm.cuh:49-89,
+ * sgemm_texld_128x128x8 in src/kernels/128x128x8_texld.cuh): when lda and ldb
+ * are multiples of 4 and A and B are 16-byte aligned (the reference's
+ * is_aligned condition), A and B are read through linear texture objects as
+ * float4 texels; otherwise -- and for k == 0, or operands too large for a
+ * linear texture -- the call runs sgemm_b200's kernels, as the reference
+ * falls back to its plain-load kernel.  Results equal sgemm_b200's bit for
+ * bit.  The texture objects are created per call and destroyed once the
+ * call's kernel has finished, without the call waiting for it. */
+int sgemm_b200_texld(int m, int n, int k,
+                     const float* alpha,
+                     const float* A, int lda,
+                     const float* B, int ldb,
+                     const float* beta,
+                     float* C, int ldc,
+                     sgemm_b200_stream_t stream);
+
 /* Replaces sgemm_basic() at src/sgemm.cuh:92-113 (kernel_basic,
  * src/kernels/basic.cuh:1-26): one thread per C element, sequential
  * accumulation, C always read.  Kept for the reference's test semantics. */

@@ -121,6 +121,7 @@ def _declare(lib: ctypes.CDLL) -> None:
     d("sgemm_b200_abi_version", _I, [])
     d("sgemm_b200_packs", _I, [_I, _I, _I, _P, _I, _P, _I])
     d("sgemm_b200_basic", _I, _GEMM_ARGS + [_P])
+    d("sgemm_b200_texld", _I, _GEMM_ARGS + [_P])
     d("sgemm_b200_split_workspace_size", ctypes.c_size_t, [_I, _I, _I, _I])
     d("sgemm_b200_split", _I, [_I] + _GEMM_ARGS + [_P, ctypes.c_size_t, _P])
     d("sgemm_b200_gemm", _I, [_I] + _GEMM_ARGS + [_P])
@@ -246,6 +247,18 @@ def sgemm(A, B, C, alpha: float = 1.0, beta: float = 0.0, stream=None, config: i
     pc, ldc = _mat(C, "C")
     _check(lib().sgemm_b200_with_config(config, m, n, k, _f(alpha), pa, lda, pb, ldb, _f(beta),
                                         pc, ldc, _stream_ptr(stream)), "sgemm_b200")
+
+
+def sgemm_texld(A, B, C, alpha: float = 1.0, beta: float = 0.0, stream=None) -> None:
+    """The texture-fetch loader (the reference's pre-Ampere path): same result
+    as sgemm(), A and B read through texture objects when aligned."""
+    m, k = A.shape
+    n = B.shape[1]
+    pa, lda = _mat(A, "A")
+    pb, ldb = _mat(B, "B")
+    pc, ldc = _mat(C, "C")
+    _check(lib().sgemm_b200_texld(m, n, k, _f(alpha), pa, lda, pb, ldb, _f(beta), pc, ldc,
+                                  _stream_ptr(stream)), "sgemm_b200_texld")
 
 
 def sgemm_basic(A, B, C, alpha: float = 1.0, beta: float = 0.0, stream=None) -> None:
