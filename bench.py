@@ -571,13 +571,13 @@ def _grouped_leg(torch, sg, sms, sm_mhz, hbm_gbs, count=512):
     t_tuned = timed(lambda: plan.launch(use_graph=True), 7)
     tinfo = plan.info()
     plan.close()
-    # a workload where the tuner's choice matters: 32 problems of 256 x 256 x
-    # 32768 (256 tiles for 444 resident CTA slots, so split-K pays)
+    # a workload where the tuner's choice matters: 16 problems of 128 x 128 x
+    # 65536 (32 tiles for 444 resident CTA slots, so split-K pays)
     kspecs = []
-    for i in range(32):
-        A = torch.empty((256, 32768), device="cuda")
-        B = torch.empty((32768, 256), device="cuda")
-        C = torch.zeros((256, 256), device="cuda")
+    for i in range(16):
+        A = torch.empty((128, 65536), device="cuda")
+        B = torch.empty((65536, 128), device="cuda")
+        C = torch.zeros((128, 128), device="cuda")
         sg.fill_random(A, 1200 + i, 1, 0)
         sg.fill_random(B, 1200 + i, 2, 0)
         kspecs.append((A, B, C, 1.0, 0.0))
@@ -594,8 +594,8 @@ def _grouped_leg(torch, sg, sms, sm_mhz, hbm_gbs, count=512):
     kinfo = plan.info()
     plan.close()
     os.unlink(ktuned)
-    kflop = 32 * 2.0 * 256 * 256 * 32768
-    k_heavy = {"workload": "32 problems of 256 x 256 x 32768, alpha=1 beta=0",
+    kflop = 16 * 2.0 * 128 * 128 * 65536
+    k_heavy = {"workload": "16 problems of 128 x 128 x 65536, alpha=1 beta=0",
                "default_ms": round(tk_default, 3), "tuned_ms": round(tk_tuned, 3),
                "default_gflops": round(kflop / tk_default * 1e-6, 1),
                "tuned_gflops": round(kflop / tk_tuned * 1e-6, 1),
@@ -870,14 +870,20 @@ def run(args):
     if rank == 0 and world == 1 and not args.skip_grouped:
         del A, B, C, C0, flush
         torch.cuda.empty_cache()
-        result["grouped"] = _grouped_leg(torch, sg, sms, sm_max, peaks["hbm_gbs"],
-                                         args.grouped_problems)
+        try:
+            result["grouped"] = _grouped_leg(torch, sg, sms, sm_max, peaks["hbm_gbs"],
+                                             args.grouped_problems)
+        except Exception as e:  # an auxiliary leg reports its failure, never hides the line
+            result["grouped"] = {"error": str(e)}
         torch.cuda.empty_cache()
     if rank == 0 and world == 1 and not args.skip_serving:
-        result["serving"] = _serving_leg(sg, [500.0, 1000.0, 2000.0, 4000.0],
-                                         args.serving_requests,
-                                         sms * 256 * sm_max * 1e-3,
-                                         peaks["bf16_tflops"] * 1e3 / 6, peaks["hbm_gbs"])
+        try:
+            result["serving"] = _serving_leg(sg, [500.0, 1000.0, 2000.0, 4000.0],
+                                             args.serving_requests,
+                                             sms * 256 * sm_max * 1e-3,
+                                             peaks["bf16_tflops"] * 1e3 / 6, peaks["hbm_gbs"])
+        except Exception as e:  # an auxiliary leg reports its failure, never hides the line
+            result["serving"] = {"error": str(e)}
     if rank == 0:
         print(json.dumps(result))
     if dist is not None:

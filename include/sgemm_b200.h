@@ -381,6 +381,11 @@ int sgemm_b200_selftest_wait_timeout(int limit_us, sgemm_b200_stream_t stream);
 int sgemm_b200_last_status(void);
 const char* sgemm_b200_status_string(int status);
 
+/* Detail of the most recent failure on the calling thread: the failing CUDA
+ * call's error name and message, or the rejected tensor-map parameters; "" if
+ * nothing has failed yet.  Not cleared by successful calls. */
+const char* sgemm_b200_last_error_detail(void);
+
 /* Library version string. */
 const char* sgemm_b200_version(void);
 

@@ -232,6 +232,10 @@ def ref_variant(v: int) -> ctypes.CDLL:
         l.ref_sgemm.argtypes = [_I, _I, _I, fp, v_, _I, v_, _I, fp, v_, _I]
         l.ref_variant.restype = _I
         assert l.ref_variant() == v
+        if v == 4:
+            l.ref_probe_reset.restype = _I
+            l.ref_probe_read.restype = _I
+            l.ref_probe_read.argtypes = [ctypes.c_void_p]
         _ref_variants[v] = l
     return _ref_variants[v]
 
@@ -245,3 +249,18 @@ def ref_sgemm_variant(v: int, A, B, C, alpha: float, beta: float) -> None:
     b = ctypes.c_float(beta)
     ref_variant(v).ref_sgemm(m, n, k, ctypes.byref(a), A.data_ptr(), A.stride(0), B.data_ptr(),
                              B.stride(0), ctypes.byref(b), C.data_ptr(), C.stride(0))
+
+
+def ref_shared_addresses(A, B, C, alpha: float, beta: float) -> list:
+    """Run variant 4 of the reference's sgemm() once and return the shared
+    addresses its address-conversion macro produced for block (0, 0) thread 0,
+    in call order."""
+    import torch
+    l = ref_variant(4)
+    assert l.ref_probe_reset() == 0
+    ref_sgemm_variant(4, A, B, C, alpha, beta)
+    torch.cuda.synchronize()
+    out = (ctypes.c_ulonglong * 16)()
+    n = l.ref_probe_read(ctypes.addressof(out))
+    assert n >= 0
+    return [int(out[i]) for i in range(min(n, 16))]

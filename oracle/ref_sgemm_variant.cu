@@ -18,13 +18,31 @@
 //   REF_VARIANT 1: clobber on the shared LOADS only (LDS128)
 //   REF_VARIANT 2: clobber on the shared STORES only (STS128, STS32)
 //   REF_VARIANT 3: clobber on every macro
+//   REF_VARIANT 4: no clobber; the address conversion macro also records, for
+//                  block (0, 0) thread 0, each shared address it returns (in
+//                  call order, at most 16) so the host can check the kernels'
+//                  XOR double-buffer arithmetic against the real bases
 // A variant that makes the kernel agree with the oracle bit for bit names the
 // statements the compiler moved.  The benchmark's reference arm never uses
 // these builds; it runs the unmodified reference (ref_sgemm.cu).
 #include "helper_cuda ptx.h"  // the reference's macros; #pragma once keeps them from returning
 
 #ifndef REF_VARIANT
-#error "REF_VARIANT must be 1, 2 or 3"
+#error "REF_VARIANT must be 1, 2, 3 or 4"
+#endif
+
+#if REF_VARIANT == 4
+__device__ unsigned long long g_probe_addr[16];
+__device__ unsigned int g_probe_n;
+#undef CVTA_TO_SHARED_PTX
+#define CVTA_TO_SHARED_PTX(addr, smem_ptr)                                                  \
+    {                                                                                       \
+        asm volatile("cvta.to.shared.u64 %0, %1;" : "=l"(addr) : "l"(smem_ptr));             \
+        if (threadIdx.x == 0 && blockIdx.x == 0 && blockIdx.y == 0) {                       \
+            const unsigned int slot_ = atomicAdd(&g_probe_n, 1u);                           \
+            if (slot_ < 16u) g_probe_addr[slot_] = (unsigned long long)(addr);              \
+        }                                                                                   \
+    }
 #endif
 
 #if REF_VARIANT == 1 || REF_VARIANT == 3
@@ -91,4 +109,20 @@ extern "C" void ref_sgemm(int m, int n, int k, const float* alpha, float* A, int
 }
 
 extern "C" int ref_variant(void) { return REF_VARIANT; }
+
+#if REF_VARIANT == 4
+// Clear the record (before a launch) and read it back (after it): returns the
+// number of addresses recorded and copies up to 16 of them to out.
+extern "C" int ref_probe_reset(void) {
+    const unsigned int zero = 0;
+    return cudaMemcpyToSymbol(g_probe_n, &zero, sizeof(zero)) == cudaSuccess ? 0 : -1;
+}
+extern "C" int ref_probe_read(unsigned long long* out) {
+    unsigned int n = 0;
+    if (cudaMemcpyFromSymbol(&n, g_probe_n, sizeof(n)) != cudaSuccess) return -1;
+    if (cudaMemcpyFromSymbol(out, g_probe_addr, sizeof(unsigned long long) * 16) != cudaSuccess)
+        return -1;
+    return (int)n;
+}
+#endif
 

@@ -1,5 +1,6 @@
 // common.cu — status word, device cache, tensor-map encoding, argument checks,
 // and the small public utility entry points.
+#include <cstdarg>
 #include <cudaTypedefs.h>
 
 #include <cstring>
@@ -88,6 +89,11 @@ bool encode_tensor_map_2d(CUtensorMap* map, CUtensorMapDataType dtype, const voi
     CUresult r = fn(map, dtype, 2, const_cast<void*>(base), dims, strides, box, estr,
                     CU_TENSOR_MAP_INTERLEAVE_NONE, swizzle, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS)
+        note_error("cuTensorMapEncodeTiled (2-D) returned %d: dims %llu x %llu, row %llu B, "
+                   "box %u x %u", (int)r, (unsigned long long)inner_elems,
+                   (unsigned long long)outer_elems, (unsigned long long)row_stride_bytes,
+                   box_inner, box_outer);
     return r == CUDA_SUCCESS;
 }
 
@@ -104,6 +110,12 @@ bool encode_tensor_map_3d(CUtensorMap* map, CUtensorMapDataType dtype, const voi
     CUresult r = fn(map, dtype, 3, const_cast<void*>(base), dims, strides, box, estr,
                     CU_TENSOR_MAP_INTERLEAVE_NONE, swizzle, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS)
+        note_error("cuTensorMapEncodeTiled (3-D) returned %d: dims %llu x %llu x %llu, "
+                   "strides %llu %llu B, box %u x %u x %u, base %p", (int)r,
+                   (unsigned long long)inner, (unsigned long long)mid, (unsigned long long)outer,
+                   (unsigned long long)mid_stride_bytes, (unsigned long long)outer_stride_bytes,
+                   box_inner, box_mid, box_outer, base);
     return r == CUDA_SUCCESS;
 }
 
@@ -190,6 +202,18 @@ extern "C" const char* sgemm_b200_status_string(int s) {
 extern "C" const char* sgemm_b200_version(void) { return "sgemm_b200 0.2.0 (sm_100a)"; }
 
 extern "C" int sgemm_b200_abi_version(void) { return SGEMM_B200_ABI_VERSION; }
+
+namespace sgb {
+static thread_local char g_error_detail[512] = "";
+void note_error(const char* fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    std::vsnprintf(g_error_detail, sizeof(g_error_detail), fmt, ap);
+    va_end(ap);
+}
+}  // namespace sgb
+
+extern "C" const char* sgemm_b200_last_error_detail(void) { return sgb::g_error_detail; }
 
 extern "C" int sgemm_b200_pool_usage(size_t* used_bytes, size_t* reserved_bytes) {
     if (!used_bytes || !reserved_bytes) return SGEMM_B200_ERR_INVALID_ARG;

@@ -34,8 +34,13 @@ bool device_is_sm100();
 
 inline cudaStream_t as_stream(sgemm_b200_stream_t s) { return reinterpret_cast<cudaStream_t>(s); }
 
+// Detail of the most recent failure on this thread (read back through
+// sgemm_b200_last_error_detail): printf-style message.
+void note_error(const char* fmt, ...);
+
 inline int cuda_status(cudaError_t e) {
     if (e == cudaSuccess) return SGEMM_B200_OK;
+    note_error("%s: %s", cudaGetErrorName(e), cudaGetErrorString(e));
     if (e == cudaErrorMemoryAllocation) return SGEMM_B200_ERR_NO_MEMORY;
     return SGEMM_B200_ERR_CUDA;
 }

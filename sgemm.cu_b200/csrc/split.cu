@@ -582,7 +582,7 @@ __device__ __forceinline__ int snake_tile(int c, int r, int G) {
 }
 
 template <int PATH>
-__global__ void __maxnreg__(200) split_grouped_kernel(const GSParams gp) {
+__global__ void __launch_bounds__(THREADS, 1) split_grouped_kernel(const GSParams gp) {
     using T = Traits<PATH>;
     using L = Layout<PATH>;
     extern __shared__ uint8_t smem_raw[];
@@ -1032,6 +1032,12 @@ static int grouped_enqueue(const GroupedTables& gt, const uint8_t* d, cudaStream
     pp.a_blocks = gt.a_prefix.back();
     const int blocks = gt.a_prefix.back() + gt.b_prefix.back();
     split_prepass_grouped_kernel<PATH><<<blocks, 256, 0, stream>>>(pp);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        note_error("grouped split pre-pass launch (%d blocks): %s", blocks, cudaGetErrorString(e));
+        return cuda_status(e) == SGEMM_B200_ERR_NO_MEMORY ? SGEMM_B200_ERR_NO_MEMORY
+                                                           : SGEMM_B200_ERR_CUDA;
+    }
     GSParams gp;
     gp.probs = reinterpret_cast<const GSProblem*>(d);
     gp.tiles = reinterpret_cast<const GSTile*>(d + gt.off_tiles);
@@ -1042,7 +1048,13 @@ static int grouped_enqueue(const GroupedTables& gt, const uint8_t* d, cudaStream
     const int sms = device_info().sm_count > 0 ? device_info().sm_count : 148;
     const int grid = std::min(gp.n_tiles, sms);
     split_grouped_kernel<PATH><<<grid, THREADS, Layout<PATH>::SMEM_BYTES, stream>>>(gp);
-    return cuda_status(cudaGetLastError());
+    e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        note_error("grouped split kernel launch (%d CTAs x %d threads, %d B shared): %s", grid,
+                   THREADS, Layout<PATH>::SMEM_BYTES, cudaGetErrorString(e));
+        return SGEMM_B200_ERR_CUDA;
+    }
+    return SGEMM_B200_OK;
 }
 
 template <int PATH>

@@ -41,6 +41,10 @@ class SgemmError(RuntimeError):
     def __init__(self, status: int, what: str = ""):
         self.status = status
         msg = status_string(status) if _lib is not None else str(status)
+        if _lib is not None and status == ERR_CUDA:
+            detail = _lib.sgemm_b200_last_error_detail().decode()
+            if detail:
+                msg += f" [{detail}]"
         super().__init__(f"{what}: {msg} (status {status})" if what else msg)
 
 
@@ -151,6 +155,7 @@ def _declare(lib: ctypes.CDLL) -> None:
     d("sgemm_b200_selftest_wait_timeout", _I, [_I, _P])
     d("sgemm_b200_last_status", _I, [])
     d("sgemm_b200_status_string", ctypes.c_char_p, [_I])
+    d("sgemm_b200_last_error_detail", ctypes.c_char_p, [])
     d("sgemm_b200_version", ctypes.c_char_p, [])
     d("sgemm", None, _GEMM_ARGS)
     d("sgemm_basic", None, _GEMM_ARGS)

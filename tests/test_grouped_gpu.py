@@ -260,16 +260,16 @@ def test_bucket_stage_count_keeps_results(tmp_path, depth):
 
 
 def test_autotuner_beats_default_on_k_heavy_problems(tmp_path):
-    """32 problems of 256 x 256 x 32768: 256 tiles leave most of the GPU's
-    resident slots idle, so the default plan (no split-K) is far from the
-    tuned one, which splits K; the tuned plan is faster and its results stay
-    within FP32 accuracy (the split sums are reduced in a fixed order)."""
+    """16 problems of 128 x 128 x 65536: 32 tiles leave almost every resident
+    slot idle, so the default plan (no split-K) is far from the tuned one,
+    which splits K; the tuned plan is several times faster and its results
+    stay within FP32 accuracy (the split sums are reduced in a fixed order)."""
     torch = _torch()
     specs = []
-    for i in range(32):
-        A = torch.empty((256, 32768), device="cuda")
-        B = torch.empty((32768, 256), device="cuda")
-        C = torch.zeros((256, 256), device="cuda")
+    for i in range(16):
+        A = torch.empty((128, 65536), device="cuda")
+        B = torch.empty((65536, 128), device="cuda")
+        C = torch.zeros((128, 128), device="cuda")
         sg.fill_random(A, 1200 + i, 1, 0)
         sg.fill_random(B, 1200 + i, 2, 0)
         specs.append((A, B, C, 1.0, 0.0))
@@ -296,7 +296,7 @@ def test_autotuner_beats_default_on_k_heavy_problems(tmp_path):
     default, tuned = sg.GroupedPlan(specs), sg.GroupedPlan(specs, tuning_json=path)
     t_default, t_tuned = time_plan(default), time_plan(tuned)
     print(f"default {t_default:.3f} ms, tuned {t_tuned:.3f} ms")
-    assert t_tuned < 0.8 * t_default
+    assert t_tuned < 0.5 * t_default
     for (A, B, C, a, b) in specs[:4]:
         want = A.double() @ B.double()
         assert torch.allclose(C.double(), want, rtol=0, atol=1e-5 * want.abs().max().item())

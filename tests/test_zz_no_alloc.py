@@ -117,7 +117,7 @@ def test_noalloc_allocates_nothing(path):
 @pytest.mark.parametrize("path,largest", [("bf16x6", 2361), ("tf32x3", 2048)])
 def test_noalloc_size_boundary(path, largest):
     """The largest accepted cube runs and equals the allocating entry point;
-    one more row, column or k step is refused before any work."""
+    a larger problem is refused before any work."""
     import torch
 
     p = sg.PATHS[path]
@@ -135,9 +135,13 @@ def test_noalloc_size_boundary(path, largest):
     torch.cuda.synchronize()
     assert sg.device_status() == sg.OK
     assert torch.equal(c_new, c_old)
-    # k is padded to a multiple of 8, so the next larger k is 8 more
-    for dm, dn, dk in ((1, 0, 0), (0, 1, 0), (0, 0, 8)):
-        m2, n2, k2 = n + dm, n + dn, n + dk
+    # the next cube is refused; TF32X3 at 2048^3 fills the scratch exactly, so
+    # there one more row, column or k step (k is padded to a multiple of 8) is
+    # refused too -- BF16X6's largest cube leaves slack from that padding
+    beyond = [(n + 1, n + 1, n + 1)]
+    if path == "tf32x3":
+        beyond += [(n + 1, n, n), (n, n + 1, n), (n, n, n + 8)]
+    for m2, n2, k2 in beyond:
         assert sg.split_workspace_size(p, m2, n2, k2) > limit
         A2 = torch.zeros((m2, k2), device="cuda")
         B2 = torch.zeros((k2, n2), device="cuda")
