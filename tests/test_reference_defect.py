@@ -1,0 +1,191 @@
+"""Root cause of the reference's sgemm_128x128x8 defect when built for sm_100a.
+
+Recorded finding (tests/test_oracle.py, test_reference_128x128x8_defect_*):
+the reference's sgemm_128x128x8 returns wrong values whenever its main loop
+runs (k > 8), while sgemm_128x256x8 is correct.  The mechanism, pinned here:
+
+Both kernels double-buffer their shared tiles by XOR-ing a thread's shared
+address with the buffer size (128x128x8.cuh:186-187,256-259: A ^ 8192, B ^
+4096; 128x256x8.cuh:120-121,244-247: both ^ 8192) and then adding the row and
+column offsets of each load or store *after* the XOR.  The storing thread and
+the loading thread of an element start from different bases, so they meet on
+the same address in the second buffer only if the XOR commutes with those
+offsets -- which holds when the shared array starts at the 16 KB boundary its
+`__align__(2 * smem_a_size * sizeof(float))` requests (128x128x8.cuh:32-33,
+128x256x8.cuh:25-26).
+If the array starts elsewhere, sgemm_128x128x8's B tile (4 KB buffers, XOR
+4096) is stored and loaded at different addresses for some elements in every
+odd k block; sgemm_128x256x8's layout stays consistent at the same bases.
+
+The CPU tests restate both kernels' shared-memory index arithmetic (file:line
+cited per term) and count, for a given array base, the elements whose writer
+and reader disagree.  The GPU test reads the base the kernels really see (a
+build of the unmodified reference whose address-conversion macro also records
+its results, oracle/ref_sgemm_variant.cu variant 4) and checks that the model
+predicts the defect for exactly the kernel that shows it.  A second finding
+rules out the other suspect: giving every inline-PTX macro a "memory" clobber
+(variants 1-3) leaves the wrong results unchanged, so the compiler moving
+shared loads or stores across the barrier is not the cause.
+"""
+import numpy as np
+import pytest
+
+import oracle
+
+
+def mismatches_128x128x8(a0: int, b0: int) -> int:
+    """Elements of the second buffer whose store address differs from their
+    load address, for A at shared address a0 and B at b0.
+
+    A (src/kernels/128x128x8.cuh:93-97 store base, 128 STS128, 151-161 load
+    base, 211-227 loads): thread t stores
+    k = t % 8, m = 4 (t / 8) + 0..3 as one 16-byte STS at
+    (a0 + 4 (4 (t/8) + 132 (t%8))) ^ 8192; lane l of warp w loads 16 bytes at
+    ((a0 + 4 (4 lmy + wmy)) ^ 8192) + 4 (132 p + s), s in {0, 16}, with
+    lmy = (l/2) % 4, wmy = 32 (w/2).
+    B (:99-108 store base, 138-140 and 247-251 STS32): thread t stores
+    k = t / 32, n = t % 32 + 32 i (i < 4)
+    as 4-byte STS at ((b0 + 4 (t%32 + 128 (t/32))) ^ 4096) + 128 i; lane l of
+    warp w loads 16 bytes at ((b0 + 4 (4 lmx + wmx)) ^ 4096) + 4 (128 p + s),
+    s in {0, 32}, with lmx = 2 (l/8) + l % 2, wmx = 64 (w % 2)."""
+    bad = 0
+    W = {}
+    for t in range(256):
+        k, m = t % 8, 4 * (t // 8)
+        W[(k, m)] = (a0 + (m + k * 132) * 4) ^ 8192
+    for w in range(8):
+        for l in range(32):
+            lmy, wmy = (l // 2) % 4, 32 * (w // 2)
+            x = a0 + (4 * lmy + wmy) * 4
+            for p in range(8):
+                for s in (0, 16):
+                    bad += W[(p, 4 * lmy + wmy + s)] != (x ^ 8192) + (p * 132 + s) * 4
+    W = {}
+    for t in range(256):
+        k, c = t // 32, t % 32
+        x = b0 + (c + k * 128) * 4
+        for i in range(4):
+            W[(k, c + 32 * i)] = (x ^ 4096) + i * 128
+    for w in range(8):
+        for l in range(32):
+            lmx, wmx = 2 * (l // 8) + l % 2, 64 * (w % 2)
+            x = b0 + (4 * lmx + wmx) * 4
+            for p in range(8):
+                for s in (0, 32):
+                    r = (x ^ 4096) + (p * 128 + s) * 4
+                    for j in range(4):
+                        bad += W[(p, 4 * lmx + wmx + s + j)] != r + 4 * j
+    return bad
+
+
+def mismatches_128x256x8(a0: int, b0: int) -> int:
+    """The same count for sgemm_128x256x8 (src/kernels/128x256x8.cuh:71-79
+    store bases, 91-112 and 207-221 cp.async stores, 127-135 load bases): A
+    stored as 4-byte cp.async at
+    ((a0 + 4 (t/8 + 132 (t%8))) ^ 8192) + 128 i (k = t % 8, m = t/8 + 32 i),
+    loaded 16 bytes at ((a0 + 4 (4 lmy + wmy)) ^ 8192) + 4 (132 p + s),
+    s in {0, 16, 32, 48}, wmy = 64 (w/4); B stored at
+    ((b0 + 4 (t%128 + 256 (t/128))) ^ 8192) + 4 (512 i + 128 h)
+    (k = t/128 + 2 i, n = t % 128 + 128 h), loaded 16 bytes at
+    ((b0 + 4 (4 lmx + wmx)) ^ 8192) + 4 (256 p + s), s in {0, 32},
+    wmx = 64 (w % 4)."""
+    bad = 0
+    W = {}
+    for t in range(256):
+        k, m = t % 8, t // 8
+        x = a0 + (m + k * 132) * 4
+        for i in range(4):
+            W[(k, m + 32 * i)] = (x ^ 8192) + i * 128
+    for w in range(8):
+        for l in range(32):
+            lmy, wmy = (l // 2) % 4, 64 * (w // 4)
+            x = a0 + (4 * lmy + wmy) * 4
+            for p in range(8):
+                for s in (0, 16, 32, 48):
+                    r = (x ^ 8192) + (p * 132 + s) * 4
+                    for j in range(4):
+                        bad += W[(p, 4 * lmy + wmy + s + j)] != r + 4 * j
+    W = {}
+    for t in range(256):
+        c, k0 = t % 128, t // 128
+        x = b0 + (c + k0 * 256) * 4
+        for i in range(4):
+            for h in range(2):
+                W[(k0 + 2 * i, c + 128 * h)] = (x ^ 8192) + (i * 2 * 256 + h * 128) * 4
+    for w in range(8):
+        for l in range(32):
+            lmx, wmx = 2 * (l // 8) + l % 2, 64 * (w % 4)
+            x = b0 + (4 * lmx + wmx) * 4
+            for p in range(8):
+                for s in (0, 32):
+                    r = (x ^ 8192) + (p * 256 + s) * 4
+                    for j in range(4):
+                        bad += W[(p, 4 * lmx + wmx + s + j)] != r + 4 * j
+    return bad
+
+
+def test_buffers_agree_at_the_requested_alignment():
+    # the array at a 16 KB boundary (what __align__ requests): both kernels'
+    # stores and loads of the second buffer meet
+    for base in (0, 16384, 5 * 16384):
+        assert mismatches_128x128x8(base, base + 16384) == 0
+        assert mismatches_128x256x8(base, base + 16384) == 0
+
+
+def test_128x128x8_breaks_off_the_alignment_128x256x8_does_not():
+    # the array 1 KB or 2 KB past a 16 KB boundary: sgemm_128x128x8's B
+    # buffers (XOR 4096) disagree, sgemm_128x256x8's layout still agrees
+    for base in (1024, 2048, 16384 + 1024):
+        assert mismatches_128x128x8(base, base + 16384) > 0
+        assert mismatches_128x256x8(base, base + 16384) == 0
+
+
+@pytest.mark.gpu
+def test_recorded_bases_explain_the_defect():
+    """The bases the kernels really see on this GPU, recorded by the
+    instrumented build, and the model's prediction for them: a mismatch for
+    sgemm_128x128x8 (the kernel whose results are wrong at k > 8) and none for
+    sgemm_128x256x8 (the kernel whose results equal ours bit for bit)."""
+    import torch
+
+    found = {}
+    for size in (1000, 4096):  # the reference dispatches 128x128x8, then 128x256x8
+        A = torch.rand(size, size, device="cuda")
+        B = torch.rand(size, size, device="cuda")
+        C = torch.rand(size, size, device="cuda")
+        addrs = oracle.ref_shared_addresses(A, B, C, 1.5, 0.5)
+        kernel = oracle.ref().ref_sgemm_kernel_choice(size, size)
+        # the first two conversions of thread 0 are the A and B store bases,
+        # which for thread 0 are the A and B array starts
+        a0, b0 = addrs[0], addrs[1]
+        assert b0 - a0 == 16384
+        found[kernel] = (a0, b0)
+        print(f"size {size}: kernel {kernel}, shared base {a0:#x}")
+    a0, b0 = found[0]
+    assert mismatches_128x128x8(a0, b0) > 0
+    assert a0 % 16384 != 0  # the requested alignment did not hold
+    a1, b1 = found[1]
+    assert mismatches_128x256x8(a1, b1) == 0
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("variant", [1, 2, 3])
+def test_memory_clobbers_do_not_repair_128x128x8(variant):
+    """The reference's PTX macros given "memory" clobbers (shared loads only,
+    shared stores only, every macro): the output is as wrong as the
+    unmodified build's, so reordering across the barrier is not the cause."""
+    import torch
+
+    m = n = k = 300
+    A = oracle.fill(m, k, 6, 1, 0)
+    B = oracle.fill(k, n, 6, 2, 0)
+    C = oracle.fill(m, n, 6, 3, 0)
+    want = oracle.sgemm_basic(A, B, C, 1.5, 0.5, basic=False)
+    dA, dB = torch.from_numpy(A).cuda(), torch.from_numpy(B).cuda()
+    base = torch.from_numpy(C).cuda()
+    fixed = torch.from_numpy(C).cuda()
+    oracle.ref_sgemm(dA, dB, base, 1.5, 0.5)
+    oracle.ref_sgemm_variant(variant, dA, dB, fixed, 1.5, 0.5)
+    torch.cuda.synchronize()
+    assert not np.array_equal(base.cpu().numpy(), want)
+    assert not np.array_equal(fixed.cpu().numpy(), want)
