@@ -1,0 +1,40 @@
+"""CPU checks of bench.py's reference arm: it must time the reference's own
+sgemm() with nothing of this repository's library loaded (its inputs come from
+the oracle's host generator), and both arms must describe the workload with
+the same config except for the kernel that runs."""
+import ast
+import os
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _functions():
+    tree = ast.parse(open(os.path.join(ROOT, "bench.py")).read())
+    return {f.name: f for f in tree.body if isinstance(f, ast.FunctionDef)}
+
+
+def test_reference_arm_loads_nothing_of_the_library():
+    fns = _functions()
+    for name in ("run_reference", "_host_inputs"):
+        f = fns[name]
+        for node in ast.walk(f):
+            if isinstance(node, (ast.Import, ast.ImportFrom)):
+                mods = [a.name for a in node.names] + [getattr(node, "module", None) or ""]
+                assert not any("sgemm_b200" in m for m in mods), (name, mods)
+            if isinstance(node, ast.Name):
+                assert node.id != "sg", f"{name} uses the library binding"
+    # and every helper it calls is library-free too
+    called = {n.func.id for n in ast.walk(fns["run_reference"])
+              if isinstance(n, ast.Call) and isinstance(n.func, ast.Name)}
+    for helper in called & set(fns):
+        for node in ast.walk(fns[helper]):
+            if isinstance(node, ast.Name):
+                assert node.id != "sg", f"{helper} (called by the reference arm) uses the library"
+
+
+def test_both_arms_build_config_with_the_same_function():
+    fns = _functions()
+    for name in ("run", "run_reference"):
+        calls = [n for n in ast.walk(fns[name]) if isinstance(n, ast.Call)
+                 and isinstance(n.func, ast.Name) and n.func.id == "_config"]
+        assert calls, f"{name} does not build its config with _config"
