@@ -76,7 +76,11 @@ inline double tile_efficiency(int t) {
 
 struct GProblem {
     Operands op;
-    int tile;      // a TileShape
+    int tile;      // a TileShape: the tile of the problem's rows (all of them,
+                   // or the bulk when `rem_tile` covers a remainder strip)
+    int rem_tile;  // tile of the last rows when they are a strip of their own, else -1
+    int rem_m0;    // first row of that strip
+    int shapes;    // bit t: the problem has tiles of shape t (a map pair per shape)
     int tma;       // tensor maps valid
     int split;     // k splits
     int kbps;      // k blocks per split
@@ -86,14 +90,18 @@ struct GProblem {
     long long ws_base;  // first workspace float (split > 1)
 };
 
+// One work item: a tile of one problem (its shape, its first row and column)
+// and one k split.  tl is the tile's index within its problem (split-K
+// tickets and partials), used only when the problem is split.
 struct GItem {
-    int prob, tm, tn, ks;
+    int prob, m0, n0, ks;
+    int tile, tl;
 };
 
 struct GParams {
     const GProblem* probs;
     const GItem* items;
-    const CUtensorMap* maps;  // 2 per problem (A, B)
+    const CUtensorMap* maps;  // 6 per problem: (A, B) for each tile shape it uses
     float* ws;
     int* counters;  // [0] work ticket, [1..] split-K tile tickets
     int* status;
@@ -116,7 +124,7 @@ __device__ __forceinline__ bool run_item(const GParams& gp, const GProblem& pr, 
     const int wm = warp / C::WN, wn = warp % C::WN;
     int lm, ln;
     ffma::lane_coords(lane, lm, ln);
-    const int m0 = it.tm * C::BM, n0 = it.tn * C::BN;
+    const int m0 = it.m0, n0 = it.n0;
     const int nk = (pr.op.k + C::BK - 1) / C::BK;
     const int kb0 = it.ks * pr.kbps;
     const int kb1 = min(nk, kb0 + pr.kbps);
@@ -134,7 +142,7 @@ __device__ __forceinline__ bool run_item(const GParams& gp, const GProblem& pr, 
         for (int j = 0; j < C::TN; ++j) acc[i][j] = 0.0f;
 
     if constexpr (TMA) {
-        const CUtensorMap* tmA = gp.maps + 2 * item_prob;
+        const CUtensorMap* tmA = gp.maps + 6 * item_prob + 2 * it.tile;
         const CUtensorMap* tmB = tmA + 1;
         int issued = 0;
         auto issue = [&](int j) {
@@ -200,7 +208,7 @@ __device__ __forceinline__ bool run_item(const GParams& gp, const GProblem& pr, 
     // ---- split-K: publish the partial, the last split of the tile reduces.
     constexpr int NQ = C::TM * C::TN / 4;
     constexpr int TILE = C::BM * C::BN;
-    const int tile_local = it.tm * pr.tiles_n + it.tn;
+    const int tile_local = it.tl;
     float4* tile_ws = reinterpret_cast<float4*>(gp.ws + pr.ws_base +
                                                 (long long)tile_local * pr.split * TILE);
     float4* mine = tile_ws + (long long)it.ks * (TILE / 4);
@@ -268,11 +276,11 @@ __global__ void __launch_bounds__(THREADS, (S == 3 ? 3 : 2)) grouped_kernel(cons
         const GItem it = gp.items[idx];
         const GProblem& pr = gp.probs[it.prob];
         bool ok;
-        if (pr.tile == kTileTall) {
+        if (it.tile == kTileTall) {
             ok = pr.tma ? run_item<CfgT<S>, true, S>(gp, pr, it, it.prob, smem, full_bar, g, &last_s)
                         : run_item<CfgT<S>, false, S>(gp, pr, it, it.prob, smem, full_bar, g,
                                                       &last_s);
-        } else if (pr.tile == kTileSkinny) {
+        } else if (it.tile == kTileSkinny) {
             ok = pr.tma ? run_item<CfgS<S>, true, S>(gp, pr, it, it.prob, smem, full_bar, g, &last_s)
                         : run_item<CfgS<S>, false, S>(gp, pr, it, it.prob, smem, full_bar, g,
                                                       &last_s);
@@ -458,29 +466,51 @@ static int make_schedule(const sgemm_b200_problem* probs, int count, const Table
         g.op.C = q.C;
         g.op.vec_c = (q.ldc % 4 == 0) && (reinterpret_cast<uintptr_t>(q.C) % 16 == 0);
         const Choice ch = table.c[bucket_of(q.m, q.n, q.k)];
-        g.tile = ch.tile;
-        {
-            // Problem geometry: a problem a few rows tall (the 32 x 128 tile)
-            // or one whose edges fit the other 8 x 8 tile better loses less
-            // work to zero padding on that tile.
-            auto cost = [&](int t) {
-                return double(div_up(q.m, tile_bm(t)) * tile_bm(t)) *
-                       double(div_up(q.n, tile_bn(t)) * tile_bn(t)) / tile_efficiency(t);
-            };
-            int best = ch.tile;
-            for (int t : {kTileTall, kTileWide, kTileSkinny})
-                if (cost(t) < 0.98 * cost(ch.tile) && cost(t) < cost(best)) best = t;
-            g.tile = best;
-        }
-        const int bm = tile_bm(g.tile), bn = tile_bn(g.tile);
-        g.tma = tma_ok(q) ? 1 : 0;
+        // Padded area per unit efficiency of covering `rows` rows with tile t.
+        auto area = [&](int rows, int t) {
+            return double(div_up(rows, tile_bm(t)) * tile_bm(t)) *
+                   double(div_up(q.n, tile_bn(t)) * tile_bn(t)) / tile_efficiency(t);
+        };
+        // Problem geometry: a problem a few rows tall (the 32 x 128 tile) or
+        // one whose edges fit the other 8 x 8 tile better loses less work to
+        // zero padding on that tile.
+        int best = ch.tile;
+        for (int t : {kTileTall, kTileWide, kTileSkinny})
+            if (area(q.m, t) < 0.98 * area(q.m, ch.tile) && area(q.m, t) < area(q.m, best)) best = t;
+        g.tile = best;
+        g.rem_tile = -1;
+        g.rem_m0 = q.m;
         const int nk = div_up(q.k, 32);
         int split = std::max(1, std::min(ch.split, nk));
         g.kbps = nk > 0 ? div_up(nk, split) : 0;
         if (g.kbps > 0) split = div_up(nk, g.kbps);  // no empty splits
         g.split = split;
         g.depth = ch.depth;
-        const int tm = q.m > 0 ? div_up(q.m, bm) : 0;
+        if (split == 1 && q.m > 0 && q.n > 0) {
+            // Rows may also be covered by two tiles: the whole tiles of a
+            // taller shape, then the leftover rows as a strip of a shorter
+            // one (every element still runs its whole k-ordered chain in one
+            // item, so the result is the same).  Taken when it pads at least
+            // 2% less than the single tile.
+            double best_area = area(q.m, best);
+            for (int t : {kTileTall, kTileWide})
+                for (int u : {kTileWide, kTileSkinny}) {
+                    if (tile_bm(u) >= tile_bm(t)) continue;
+                    const int bulk = q.m / tile_bm(t) * tile_bm(t);
+                    if (bulk == 0 || bulk == q.m) continue;
+                    const double a = area(bulk, t) + area(q.m - bulk, u);
+                    if (a < 0.98 * best_area) {
+                        best_area = a;
+                        g.tile = t;
+                        g.rem_tile = u;
+                        g.rem_m0 = bulk;
+                    }
+                }
+        }
+        g.tma = tma_ok(q) ? 1 : 0;
+        g.shapes = (1 << g.tile) | (g.rem_tile >= 0 ? 1 << g.rem_tile : 0);
+        const int bm = tile_bm(g.tile), bn = tile_bn(g.tile);
+        const int tm = q.m > 0 ? div_up(g.rem_m0, bm) : 0;
         const int tn = q.n > 0 ? div_up(q.n, bn) : 0;
         g.tiles_n = tn;
         g.cnt_base = sc.tickets;
@@ -489,15 +519,23 @@ static int make_schedule(const sgemm_b200_problem* probs, int count, const Table
             sc.tickets += tm * tn;
             sc.ws_floats += (long long)tm * tn * split * bm * bn;
         }
-        sc.tiles += tm * tn;
+        // cost ~ FMAs of the item plus a fixed pipeline fill / epilogue term
+        auto add = [&](int tile, int m0, int n0, int tl, int ks) {
+            const int kb = std::min(g.kbps, nk - ks * g.kbps);
+            const double c = double(tile_bm(tile)) * tile_bn(tile) * (std::max(kb, 0) + 6) * 32;
+            items.push_back({GItem{i, m0, n0, ks, tile, tl}, c});
+        };
         for (int a = 0; a < tm; ++a)
             for (int b = 0; b < tn; ++b)
-                for (int s = 0; s < split; ++s) {
-                    const int kb = std::min(g.kbps, nk - s * g.kbps);
-                    // cost ~ FMAs of the item plus a fixed pipeline fill / epilogue term
-                    const double c = double(bm) * bn * (std::max(kb, 0) + 6) * 32;
-                    items.push_back({GItem{i, a, b, s}, c});
-                }
+                for (int ks = 0; ks < split; ++ks) add(g.tile, a * bm, b * bn, a * tn + b, ks);
+        sc.tiles += tm * tn;
+        if (g.rem_tile >= 0) {  // the remainder strip (split == 1 only)
+            const int rbm = tile_bm(g.rem_tile), rbn = tile_bn(g.rem_tile);
+            const int rtm = div_up(q.m - g.rem_m0, rbm), rtn = div_up(q.n, rbn);
+            for (int a = 0; a < rtm; ++a)
+                for (int b = 0; b < rtn; ++b) add(g.rem_tile, g.rem_m0 + a * rbm, b * rbn, 0, 0);
+            sc.tiles += rtm * rtn;
+        }
     }
     std::stable_sort(items.begin(), items.end(),
                      [](const Weighted& x, const Weighted& y) { return x.cost > y.cost; });
@@ -505,6 +543,22 @@ static int make_schedule(const sgemm_b200_problem* probs, int count, const Table
     for (size_t i = 0; i < items.size(); ++i) sc.items[i] = items[i].it;
     *out = std::move(sc);
     return SGEMM_B200_OK;
+}
+
+// The tensor maps of one problem: an (A, B) pair for each tile shape it uses,
+// at maps[2 * shape] and maps[2 * shape + 1] (six slots per problem).
+static bool encode_problem_maps(const GProblem& g, CUtensorMap* maps) {
+    for (int t = 0; t < 3; ++t) {
+        if (!(g.shapes & (1 << t))) continue;
+        if (!encode_tensor_map_2d(&maps[2 * t], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, g.op.A,
+                                  (uint64_t)g.op.k, (uint64_t)g.op.m, (uint64_t)g.op.lda * 4, 32,
+                                  tile_bm(t), CU_TENSOR_MAP_SWIZZLE_128B) ||
+            !encode_tensor_map_2d(&maps[2 * t + 1], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, g.op.B,
+                                  (uint64_t)g.op.n, (uint64_t)g.op.k, (uint64_t)g.op.ldb * 4,
+                                  tile_bn(t), 32, CU_TENSOR_MAP_SWIZZLE_NONE))
+            return false;
+    }
+    return true;
 }
 
 // The kernels' dynamic shared-memory attribute, once per device (attributes
@@ -550,18 +604,11 @@ static int build_plan(const sgemm_b200_problem* probs, int count, const Table& t
     plan->ws_floats = (size_t)sc.ws_floats;
     plan->n_counters = 1 + sc.tickets;
 
-    std::vector<CUtensorMap> maps(2 * (size_t)std::max(count, 1));
+    std::vector<CUtensorMap> maps(6 * (size_t)std::max(count, 1));
     std::memset(maps.data(), 0, maps.size() * sizeof(CUtensorMap));
     for (int i = 0; i < count; ++i) {
         const GProblem& g = sc.probs[i];
-        if (!g.tma) continue;
-        const int bm = tile_bm(g.tile), bn = tile_bn(g.tile);
-        if (!encode_tensor_map_2d(&maps[2 * i], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, g.op.A,
-                                  (uint64_t)g.op.k, (uint64_t)g.op.m, (uint64_t)g.op.lda * 4, 32,
-                                  bm, CU_TENSOR_MAP_SWIZZLE_128B) ||
-            !encode_tensor_map_2d(&maps[2 * i + 1], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, g.op.B,
-                                  (uint64_t)g.op.n, (uint64_t)g.op.k, (uint64_t)g.op.ldb * 4, bn,
-                                  32, CU_TENSOR_MAP_SWIZZLE_NONE)) {
+        if (g.tma && !encode_problem_maps(g, &maps[6 * (size_t)i])) {
             free_plan(plan);
             return SGEMM_B200_ERR_CUDA;
         }
@@ -692,31 +739,23 @@ int arena_launch(Arena* a, const sgemm_b200_problem* probs, int count, cudaStrea
     // first capacities: 256 problems, 64 Ki work items (~1 MB pinned in all)
     chk(grow(&a->d_probs, &a->h_probs, &a->cap_probs, (size_t)count, stream, 256));
     chk(grow(&a->d_items, &a->h_items, &a->cap_items, sc.items.size(), stream, 1 << 16));
-    chk(grow(&a->d_maps, &a->h_maps, &a->cap_maps, 2 * (size_t)count, stream, 512));
+    chk(grow(&a->d_maps, &a->h_maps, &a->cap_maps, 6 * (size_t)count, stream, 1536));
     chk(grow<int>(&a->d_counters, nullptr, &a->cap_counters, n_counters, stream, 1024));
     chk(grow<float>(&a->d_ws, nullptr, &a->cap_ws, std::max<size_t>(sc.ws_floats, 1), stream,
                     1));
     if (e != cudaSuccess) return cuda_status(e);
     std::memcpy(a->h_probs, sc.probs.data(), sizeof(GProblem) * count);
     std::memcpy(a->h_items, sc.items.data(), sizeof(GItem) * sc.items.size());
-    std::memset(a->h_maps, 0, sizeof(CUtensorMap) * 2 * count);
+    std::memset(a->h_maps, 0, sizeof(CUtensorMap) * 6 * count);
     for (int i = 0; i < count; ++i) {
         const GProblem& g = sc.probs[i];
-        if (!g.tma) continue;
-        const int bm = tile_bm(g.tile), bn = tile_bn(g.tile);
-        if (!encode_tensor_map_2d(&a->h_maps[2 * i], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, g.op.A,
-                                  (uint64_t)g.op.k, (uint64_t)g.op.m, (uint64_t)g.op.lda * 4, 32,
-                                  bm, CU_TENSOR_MAP_SWIZZLE_128B) ||
-            !encode_tensor_map_2d(&a->h_maps[2 * i + 1], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, g.op.B,
-                                  (uint64_t)g.op.n, (uint64_t)g.op.k, (uint64_t)g.op.ldb * 4, bn,
-                                  32, CU_TENSOR_MAP_SWIZZLE_NONE))
-            return SGEMM_B200_ERR_CUDA;
+        if (g.tma && !encode_problem_maps(g, &a->h_maps[6 * (size_t)i])) return SGEMM_B200_ERR_CUDA;
     }
     chk(cudaMemcpyAsync(a->d_probs, a->h_probs, sizeof(GProblem) * count, cudaMemcpyHostToDevice,
                         stream));
     chk(cudaMemcpyAsync(a->d_items, a->h_items, sizeof(GItem) * sc.items.size(),
                         cudaMemcpyHostToDevice, stream));
-    chk(cudaMemcpyAsync(a->d_maps, a->h_maps, sizeof(CUtensorMap) * 2 * count,
+    chk(cudaMemcpyAsync(a->d_maps, a->h_maps, sizeof(CUtensorMap) * 6 * count,
                         cudaMemcpyHostToDevice, stream));
     chk(cudaMemsetAsync(a->d_counters, 0, sizeof(int) * n_counters, stream));
     if (e != cudaSuccess) return cuda_status(e);

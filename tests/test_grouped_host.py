@@ -31,19 +31,54 @@ def _tile_for(m, n, bucket_tile="tall"):
     return best
 
 
+def _area(rows, n, t):
+    bm, bn, eff = TILES[t]
+    return math.ceil(rows / bm) * bm * math.ceil(n / bn) * bn / eff
+
+
+def _tiles_for(m, n, bucket_tile="tall"):
+    """Tile count of a split-1 problem under the library's rule: the single
+    tile above, or -- when it pads at least 2% less -- the whole tiles of a
+    taller shape over the first rows plus a strip of a shorter shape over the
+    rest."""
+    if m == 0 or n == 0:
+        return 0, None
+    best = _tile_for(m, n, bucket_tile)
+    best_area = _area(m, n, best)
+    bm, bn, _ = TILES[best]
+    count, mixed = math.ceil(m / bm) * math.ceil(n / bn), None
+    for t in ("tall", "wide"):
+        for u in ("wide", "skinny"):
+            if TILES[u][0] >= TILES[t][0]:
+                continue
+            bulk = m // TILES[t][0] * TILES[t][0]
+            if bulk in (0, m):
+                continue
+            a = _area(bulk, n, t) + _area(m - bulk, n, u)
+            if a < 0.98 * best_area:
+                best_area = a
+                mixed = (t, u)
+                count = (bulk // TILES[t][0]) * math.ceil(n / TILES[t][1]) + \
+                    math.ceil((m - bulk) / TILES[u][0]) * math.ceil(n / TILES[u][1])
+    return count, mixed
+
+
 def test_schedule_default_counts():
-    shapes = [(64, 64, 64), (300, 520, 1001), (4096, 4096, 64), (1, 1, 1), (129, 257, 0)]
+    shapes = [(64, 64, 64), (300, 520, 1001), (4096, 4096, 64), (1, 1, 1), (129, 257, 0),
+              (136, 4096, 4096), (200, 4096, 4096), (16, 4096, 4096)]
     probs = sg.host_problems(shapes)
     s = sg.grouped_schedule(probs)
-    tiles = 0
-    for m, n, k in shapes:  # default bucket tile 128 x 64, adjusted per problem
-        bm, bn, _ = TILES[_tile_for(m, n)]
-        tiles += math.ceil(m / bm) * math.ceil(n / bn)
+    tiles = sum(_tiles_for(m, n)[0] for m, n, _ in shapes)
     assert s["tiles"] == tiles
     assert s["work_items"] == tiles  # no split-K by default: results equal the plain path
     assert s["workspace_bytes"] == 0
     # the rule moves some of these off the default tile
-    assert [_tile_for(m, n) for m, n, _ in shapes] == ["tall", "wide", "tall", "skinny", "wide"]
+    assert [_tile_for(m, n) for m, n, _ in shapes[:5]] == ["tall", "wide", "tall", "skinny",
+                                                           "wide"]
+    # tall-skinny serving requests: 136 rows as one 128-row tile plus a strip
+    # of 32-row tiles instead of two 64-row tiles
+    assert _tiles_for(136, 4096)[1] == ("tall", "skinny")
+    assert _tiles_for(16, 4096)[1] is None
 
 
 def test_schedule_ignores_table_for_other_device(tmp_path):
