@@ -80,9 +80,11 @@ def _memory_state():
 def test_noalloc_allocates_nothing(path):
     """The property that defines the entry point: a call leaves the library's
     own pool, torch's allocator and the device's free memory as they were.
-    A first call is made before measuring, so that one-time costs that are not
-    allocations by the call (loading the kernels' code onto the device, the
-    symbol lookup) do not show; the k == 0 and beta == 0 routes are covered."""
+    Each route (beta != 0, beta == 0, and k == 0, which runs a plain-path
+    kernel) is called once before measuring, so that one-time costs that are
+    not allocations by the call do not show: CUDA loads a kernel's code onto
+    the device the first time it is launched (2 MiB of device memory in a
+    fresh process), and the first call looks up the scratch array's address."""
     import torch
 
     m, n, k = 640, 384, 1000
@@ -91,7 +93,12 @@ def test_noalloc_allocates_nothing(path):
     C = oracle.fill(m, n, 41, 3, 0)
     dA, dB = torch.from_numpy(A).cuda(), torch.from_numpy(B).cuda()
     outs = [torch.from_numpy(C).cuda() for _ in range(4)]
-    assert _call_noalloc(path, dA, dB, outs[0], 1.5, 0.5) == sg.OK  # warm-up
+    # warm-up of every route measured below
+    assert _call_noalloc(path, dA, dB, outs[0], 1.5, 0.5) == sg.OK
+    warm = torch.from_numpy(C).cuda()
+    assert _call_noalloc(path, dA, dB, warm, 1.0, 0.0) == sg.OK
+    assert _call_noalloc(path, dA[:, :0], dB[:0, :], warm, 1.5, 0.5) == sg.OK
+    del warm
     before = _memory_state()
     assert _call_noalloc(path, dA, dB, outs[1], 1.5, 0.5) == sg.OK
     assert _call_noalloc(path, dA, dB, outs[2], 1.0, 0.0) == sg.OK  # beta == 0: C not read
