@@ -33,7 +33,7 @@ extern "C" {
  * its parameters or their meaning (new entry points keep it); a caller
  * compiled against one header can compare it with sgemm_b200_abi_version()
  * at run time. */
-#define SGEMM_B200_ABI_VERSION 3
+#define SGEMM_B200_ABI_VERSION 2
 int sgemm_b200_abi_version(void);
 
 /* cudaStream_t without pulling in the CUDA headers: the ABI takes it as an

@@ -56,10 +56,6 @@ typedef struct {
     /* fault injection for tests (0 = off) */
     int inject_alloc_failure_every;  /* every Nth admission fails as out-of-memory */
     int inject_batch_delay_ms;       /* host delay before each batch launch */
-    /* Requests of at least this many GFLOP (2*m*n*k / 1e9) run in a batch of
-     * their own; 0 = batch everything together.  A batch completes as a
-     * whole, so a small request batched with a large one waits for it. */
-    double solo_gflop;
 } sgemm_b200_server_config;
 
 typedef struct {

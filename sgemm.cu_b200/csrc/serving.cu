@@ -460,20 +460,12 @@ static void worker_loop(Server* s) {
         if (free_slot >= 0 && !s->ready.empty()) {
             Slot& sl = s->slots[free_slot];
             const bool gpu_idle = s->in_flight == 0;
-            // A request of at least solo_gflop runs in a batch of its own: the
-            // batch ends before it when it is not first, and right after it.
-            auto solo = [&](const Request* r) {
-                return s->cfg.solo_gflop > 0 &&
-                       2.0 * r->m * (double)r->n * r->k * 1e-9 >= s->cfg.solo_gflop;
-            };
             while (!s->ready.empty() && (int)sl.batch.size() < s->cfg.max_batch) {
                 Request* r = s->ready.front();
                 if (!gpu_idle && r->ready && cudaEventQuery(r->ready) == cudaErrorNotReady) break;
-                if (!sl.batch.empty() && solo(r)) break;
                 s->ready.pop_front();
                 r->state = kRunning;
                 sl.batch.push_back(r);
-                if (solo(r)) break;
             }
             wait_for_operands = sl.batch.empty();
         }
@@ -571,7 +563,7 @@ extern "C" int sgemm_b200_serving_workload(int n_requests, double rate, uint64_t
 extern "C" int sgemm_b200_server_create(sgemm_b200_server** out,
                                         const sgemm_b200_server_config* cfg) {
     if (!out || !cfg || cfg->slots < 1 || cfg->max_batch < 1 || cfg->hbm_budget_bytes == 0 ||
-        cfg->path < 0 || cfg->path > 2 || !(cfg->solo_gflop >= 0))
+        cfg->path < 0 || cfg->path > 2)
         return SGEMM_B200_ERR_INVALID_ARG;
     if (!sgb::device_is_sm100()) return SGEMM_B200_ERR_UNSUPPORTED;
     auto* srv = new sgemm_b200_server();

@@ -66,7 +66,6 @@ class ServerConfig(ctypes.Structure):
         ("hbm_budget_bytes", ctypes.c_size_t), ("slots", ctypes.c_int),
         ("max_batch", ctypes.c_int), ("path", ctypes.c_int), ("keep_results", ctypes.c_int),
         ("inject_alloc_failure_every", ctypes.c_int), ("inject_batch_delay_ms", ctypes.c_int),
-        ("solo_gflop", ctypes.c_double),
     ]
 
 
@@ -103,7 +102,7 @@ class TraceRecord(ctypes.Structure):
 _lib: Optional[ctypes.CDLL] = None
 
 # The C ABI version this binding was written against (SGEMM_B200_ABI_VERSION).
-ABI_VERSION = 3
+ABI_VERSION = 2
 
 _I = ctypes.c_int
 _P = ctypes.c_void_p
@@ -496,10 +495,10 @@ class Server:
 
     def __init__(self, hbm_budget_bytes: int = 64 << 30, slots: int = 2, max_batch: int = 32,
                  path="plain", keep_results: bool = False, inject_alloc_failure_every: int = 0,
-                 inject_batch_delay_ms: int = 0, solo_gflop: float = 0.0):
+                 inject_batch_delay_ms: int = 0):
         p = PATHS[path] if isinstance(path, str) else int(path)
         self.cfg = ServerConfig(hbm_budget_bytes, slots, max_batch, p, 1 if keep_results else 0,
-                                inject_alloc_failure_every, inject_batch_delay_ms, solo_gflop)
+                                inject_alloc_failure_every, inject_batch_delay_ms)
         h = ctypes.c_void_p()
         _check(lib().sgemm_b200_server_create(ctypes.byref(h), ctypes.byref(self.cfg)),
                "server_create")

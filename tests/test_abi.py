@@ -106,7 +106,7 @@ def test_select_config_keeps_its_first_signature():
     # first release exported; the beta-aware query is a separate entry point,
     # and the ABI version tells callers which header the library matches.
     l = sg.lib()
-    assert l.sgemm_b200_abi_version() == sg.ABI_VERSION == 3
+    assert l.sgemm_b200_abi_version() == sg.ABI_VERSION == 2
     for shape in ((300, 301, 299), (1024, 1024, 1024), (8192, 8192, 8192)):
         m, n, k = shape
         old = l.sgemm_b200_select_config(m, n, k, 16, k, 16, n, 16, n)
