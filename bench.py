@@ -27,7 +27,11 @@ All FP64 checks run inside the cpu_baseline leg (the oracle is the checker
 there); the other legs only collect sampled output rows.
 
 `--impl reference` runs the reference's own sgemm() (its 128x256x8 kernel at
-this size) built from its sources for sm_100a, same workload and metric.
+this size) built from its sources for sm_100a, same workload and metric, and
+at M=N=K=1024 its 128x128x8 kernel both as built (wrong results on sm_100a)
+and from the rebased test-only build that repairs it, each checked bit for
+bit.  `--ref-build rebased` times that repaired build instead of the stock one
+(a labelled comparison for sizes up to 2500; the default arm stays stock).
 
 Multi-GPU: replicas (the GEMM has no exchange step in this scope); each rank
 runs the same workload on its GPU, timing is the max over ranks.
@@ -917,11 +921,32 @@ def run_reference(args, torch, peaks, sms, local):
     except Exception as e:
         print(json.dumps({"impl": "reference", "unavailable": f"reference build missing: {e}"}))
         return
+    rebased = args.ref_build == "rebased"
+    if rebased:
+        try:
+            oracle.ref_variant(5)
+            ok = oracle.ref_rebased_premise()
+        except Exception as e:
+            print(json.dumps({"impl": "reference",
+                              "unavailable": f"rebased test-only build missing: {e}"}))
+            return
+        if not ok:
+            print(json.dumps({"impl": "reference",
+                              "unavailable": "rebased test-only build not applicable: the "
+                                             "shared array is not where its rebase assumes"}))
+            return
+
+    def ref_sgemm(a, b, c, alpha, beta):
+        if rebased:
+            oracle.ref_sgemm_variant(5, a, b, c, alpha, beta)
+        else:
+            oracle.ref_sgemm(a, b, c, alpha, beta)
+
     A, B, C = _host_inputs(torch, SIZE)
     flush = torch.empty(int(peaks.get("l2_bytes", 256 << 20)) // 4, device="cuda")
 
     def step():
-        oracle.ref_sgemm(A, B, C, ALPHA, BETA)
+        ref_sgemm(A, B, C, ALPHA, BETA)
 
     clocks = ClockSampler(local)
     clocks.start()
@@ -930,13 +955,16 @@ def run_reference(args, torch, peaks, sms, local):
     flops = 2.0 * SIZE ** 3
     t = statistics.mean(ms)
     value = flops / (t * 1e-3) * 1e-9
-    ms_e2e, h2d, d2h = _e2e(torch, lambda a, b, c: oracle.ref_sgemm(a, b, c, ALPHA, BETA),
+    ms_e2e, h2d, d2h = _e2e(torch, lambda a, b, c: ref_sgemm(a, b, c, ALPHA, BETA),
                             max(3, args.steps // 5), 2, SIZE)
     sm_max = clk.get("sm_max_mhz") or peaks.get("sm_max_mhz", 1965.0)
     peak = sms * 256 * sm_max * 1e-3
     kernel = ("reference sgemm_128x256x8 (src/sgemm.cuh:41-44)"
               if oracle.ref().ref_sgemm_kernel_choice(SIZE, SIZE) == 1
               else "reference sgemm_128x128x8 (src/sgemm.cuh:45-47)")
+    if rebased:
+        kernel += (", rebased test-only build: shared addresses moved onto the 16 KB "
+                   "boundary the kernels assume (oracle/ref_sgemm_variant.cu variant 5)")
     result = {
         "impl": "reference",
         "metric": f"plain FFMA SGEMM GFLOP/s at M=N=K={SIZE} (alpha=1.5, beta=0.5)",
@@ -959,7 +987,50 @@ def run_reference(args, torch, peaks, sms, local):
                                    "from its sources for sm_100a, on the B200, with inputs from "
                                    "the oracle's host generator"},
     }
+    if rebased:
+        result["ref_build"] = "rebased (test-only)"
+    if not rebased and not args.skip_config_1024:
+        try:
+            result["config_1024"] = _reference_config_1024(torch, oracle, args.steps,
+                                                           args.warmup)
+        except Exception as e:
+            result["config_1024"] = {"error": f"{type(e).__name__}: {e}"}
     print(json.dumps(result))
+
+
+def _reference_config_1024(torch, oracle, steps, warmup):
+    """The smallest plain config (M=N=K=1024, alpha=1, beta=0, A and B
+    uniform[-1, 1) seed 0, as the library arm's config_1024 leg) through the
+    reference.  sgemm() dispatches sgemm_128x128x8 there, whose stock sm_100a
+    build returns wrong values (its XOR double buffering assumes a 16 KB-aligned
+    shared array); the rebased test-only build of the same unmodified kernels
+    is timed beside it.  Each is checked bit for bit against the oracle, so the
+    number that is quoted as the reference's for this config is a correct one."""
+    n = 1024
+    hA = oracle.fill(n, n, SEED, 1, 0)
+    hB = oracle.fill(n, n, SEED, 2, 0)
+    hC = oracle.fill(n, n, SEED, 3, 0)
+    want = oracle.sgemm_basic(hA, hB, hC, 1.0, 0.0, basic=False).view(np.uint32)
+    A, B = torch.from_numpy(hA).cuda(), torch.from_numpy(hB).cuda()
+    flush = torch.empty((256 << 20) // 4, device="cuda")
+    out = {"alpha": 1.0, "beta": 0.0, "dist": "uniform[-1,1) seed 0",
+           "kernel": "reference sgemm_128x128x8 (src/sgemm.cuh:45-47)"}
+    builds = [("stock", oracle.ref_sgemm)]
+    if oracle.ref_rebased_premise():
+        builds.append(("rebased_test_only",
+                       lambda a, b, c, al, be: oracle.ref_sgemm_variant(5, a, b, c, al, be)))
+    else:
+        out["rebased_test_only"] = {"error": "shared array not where the rebase assumes"}
+    for name, fn in builds:
+        C = torch.from_numpy(hC).cuda()
+        fn(A, B, C, 1.0, 0.0)
+        torch.cuda.synchronize()
+        exact = bool(np.array_equal(C.cpu().numpy().view(np.uint32), want))
+        ms = _time_steps(torch, lambda: fn(A, B, C, 1.0, 0.0), steps, warmup, flush)
+        t = statistics.mean(ms)
+        out[name] = {"gflops": round(2.0 * n ** 3 / (t * 1e-3) * 1e-9, 1),
+                     "ms_per_step": round(t, 4), "bit_exact_vs_oracle": exact}
+    return out
 
 
 def main():
@@ -968,6 +1039,12 @@ def main():
     ap.add_argument("--steps", type=int, default=40)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--ref-build", choices=["stock", "rebased"], default="stock",
+                    help="reference arm only: the unmodified reference (default), or its "
+                         "rebased test-only build that repairs sgemm_128x128x8 on sm_100a "
+                         "(for labelled comparisons at sizes <= 2500)")
+    ap.add_argument("--skip-config-1024", action="store_true",
+                    help="reference arm only: skip the 1024^3 stock/rebased leg")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-split", action="store_true")

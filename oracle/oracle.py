@@ -219,8 +219,11 @@ def ref_sgemm(A, B, C, alpha: float, beta: float, basic: bool = False) -> None:
 
 
 def ref_variant(v: int) -> ctypes.CDLL:
-    """The reference's sgemm() with its PTX macros given a "memory" clobber:
-    v = 1 shared loads, 2 shared stores, 3 every macro."""
+    """The reference's sgemm() with its PTX macros redefined from outside:
+    v = 1, 2, 3 a "memory" clobber on the shared loads, the shared stores, every
+    macro; v = 4 a record of the shared addresses; v = 5 shared addresses
+    rebased onto the 16 KB boundary the kernels' XOR double buffering assumes
+    (test-only repair of sgemm_128x128x8)."""
     if v not in _ref_variants:
         path = os.path.join(HERE, "_ref", f"libref_sgemm_v{v}.so")
         if not os.path.exists(path):
@@ -241,7 +244,7 @@ def ref_variant(v: int) -> ctypes.CDLL:
 
 
 def ref_sgemm_variant(v: int, A, B, C, alpha: float, beta: float) -> None:
-    """Run a clobber variant of the reference's sgemm() on torch CUDA tensors
+    """Run variant v of the reference's sgemm() on torch CUDA tensors
     (contiguous, ldb == ldc == n as the reference requires)."""
     m, k = A.shape
     n = B.shape[1]
@@ -249,6 +252,27 @@ def ref_sgemm_variant(v: int, A, B, C, alpha: float, beta: float) -> None:
     b = ctypes.c_float(beta)
     ref_variant(v).ref_sgemm(m, n, k, ctypes.byref(a), A.data_ptr(), A.stride(0), B.data_ptr(),
                              B.stride(0), ctypes.byref(b), C.data_ptr(), C.stride(0))
+
+
+# Variant 5's rebase (ref_sgemm_variant.cu REF_REBASE): the bytes by which the
+# reference kernels' shared array sits past the 16 KB boundary they assume.
+REF_REBASE = 1024
+
+
+def ref_rebased_premise() -> bool:
+    """Whether variant 5 may run here: both reference kernels' shared array
+    starts REF_REBASE bytes past a 16 KB boundary, read from variant 4's record
+    on a small problem of each kernel (main loop included).  With any other
+    base the rebased addresses would not be the array's."""
+    import torch
+    for m, n in ((128, 128), (2560, 256)):  # sgemm_128x128x8, then sgemm_128x256x8
+        A = torch.zeros(m, 16, device="cuda")
+        B = torch.zeros(16, n, device="cuda")
+        C = torch.zeros(m, n, device="cuda")
+        addrs = ref_shared_addresses(A, B, C, 1.0, 0.0)
+        if len(addrs) < 2 or addrs[0] % 16384 != REF_REBASE or addrs[1] - addrs[0] != 16384:
+            return False
+    return True
 
 
 def ref_shared_addresses(A, B, C, alpha: float, beta: float) -> list:

@@ -15,7 +15,7 @@ def _functions():
 
 def test_reference_arm_loads_nothing_of_the_library():
     fns = _functions()
-    for name in ("run_reference", "_host_inputs"):
+    for name in ("run_reference", "_host_inputs", "_reference_config_1024"):
         f = fns[name]
         for node in ast.walk(f):
             if isinstance(node, (ast.Import, ast.ImportFrom)):

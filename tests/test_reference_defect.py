@@ -25,7 +25,11 @@ its results, oracle/ref_sgemm_variant.cu variant 4) and checks that the model
 predicts the defect for exactly the kernel that shows it.  A second finding
 rules out the other suspect: giving every inline-PTX macro a "memory" clobber
 (variants 1-3) leaves the wrong results unchanged, so the compiler moving
-shared loads or stores across the barrier is not the cause.
+shared loads or stores across the barrier is not the cause.  The repair the
+model predicts confirms it: the same unmodified kernels built with every
+shared address rebased onto the 16 KB boundary (variant 5: the address
+conversion subtracts the array's offset past the boundary, every shared load
+and store adds it back) return the oracle's results bit for bit.
 """
 import numpy as np
 import pytest
@@ -33,7 +37,12 @@ import pytest
 import oracle
 
 
-def mismatches_128x128x8(a0: int, b0: int) -> int:
+def _note(record, addr: int, nbytes: int) -> None:
+    if record is not None:
+        record.append((addr, nbytes))
+
+
+def mismatches_128x128x8(a0: int, b0: int, record=None) -> int:
     """Elements of the second buffer whose store address differs from their
     load address, for A at shared address a0 and B at b0.
 
@@ -53,19 +62,23 @@ def mismatches_128x128x8(a0: int, b0: int) -> int:
     for t in range(256):
         k, m = t % 8, 4 * (t // 8)
         W[(k, m)] = (a0 + (m + k * 132) * 4) ^ 8192
+        _note(record, W[(k, m)], 16)
     for w in range(8):
         for l in range(32):
             lmy, wmy = (l // 2) % 4, 32 * (w // 2)
             x = a0 + (4 * lmy + wmy) * 4
             for p in range(8):
                 for s in (0, 16):
-                    bad += W[(p, 4 * lmy + wmy + s)] != (x ^ 8192) + (p * 132 + s) * 4
+                    r = (x ^ 8192) + (p * 132 + s) * 4
+                    _note(record, r, 16)
+                    bad += W[(p, 4 * lmy + wmy + s)] != r
     W = {}
     for t in range(256):
         k, c = t // 32, t % 32
         x = b0 + (c + k * 128) * 4
         for i in range(4):
             W[(k, c + 32 * i)] = (x ^ 4096) + i * 128
+            _note(record, W[(k, c + 32 * i)], 4)
     for w in range(8):
         for l in range(32):
             lmx, wmx = 2 * (l // 8) + l % 2, 64 * (w % 2)
@@ -73,12 +86,13 @@ def mismatches_128x128x8(a0: int, b0: int) -> int:
             for p in range(8):
                 for s in (0, 32):
                     r = (x ^ 4096) + (p * 128 + s) * 4
+                    _note(record, r, 16)
                     for j in range(4):
                         bad += W[(p, 4 * lmx + wmx + s + j)] != r + 4 * j
     return bad
 
 
-def mismatches_128x256x8(a0: int, b0: int) -> int:
+def mismatches_128x256x8(a0: int, b0: int, record=None) -> int:
     """The same count for sgemm_128x256x8 (src/kernels/128x256x8.cuh:71-79
     store bases, 91-112 and 207-221 cp.async stores, 127-135 load bases): A
     stored as 4-byte cp.async at
@@ -96,6 +110,7 @@ def mismatches_128x256x8(a0: int, b0: int) -> int:
         x = a0 + (m + k * 132) * 4
         for i in range(4):
             W[(k, m + 32 * i)] = (x ^ 8192) + i * 128
+            _note(record, W[(k, m + 32 * i)], 4)
     for w in range(8):
         for l in range(32):
             lmy, wmy = (l // 2) % 4, 64 * (w // 4)
@@ -103,6 +118,7 @@ def mismatches_128x256x8(a0: int, b0: int) -> int:
             for p in range(8):
                 for s in (0, 16, 32, 48):
                     r = (x ^ 8192) + (p * 132 + s) * 4
+                    _note(record, r, 16)
                     for j in range(4):
                         bad += W[(p, 4 * lmy + wmy + s + j)] != r + 4 * j
     W = {}
@@ -112,6 +128,7 @@ def mismatches_128x256x8(a0: int, b0: int) -> int:
         for i in range(4):
             for h in range(2):
                 W[(k0 + 2 * i, c + 128 * h)] = (x ^ 8192) + (i * 2 * 256 + h * 128) * 4
+                _note(record, W[(k0 + 2 * i, c + 128 * h)], 4)
     for w in range(8):
         for l in range(32):
             lmx, wmx = 2 * (l // 8) + l % 2, 64 * (w % 4)
@@ -119,6 +136,7 @@ def mismatches_128x256x8(a0: int, b0: int) -> int:
             for p in range(8):
                 for s in (0, 32):
                     r = (x ^ 8192) + (p * 256 + s) * 4
+                    _note(record, r, 16)
                     for j in range(4):
                         bad += W[(p, 4 * lmx + wmx + s + j)] != r + 4 * j
     return bad
@@ -189,3 +207,56 @@ def test_memory_clobbers_do_not_repair_128x128x8(variant):
     torch.cuda.synchronize()
     assert not np.array_equal(base.cpu().numpy(), want)
     assert not np.array_equal(fixed.cpu().numpy(), want)
+
+
+# REF_REBASE of oracle/ref_sgemm_variant.cu variant 5: the array's offset past
+# the 16 KB boundary that the recorded bases show on sm_100a
+REBASE = oracle.REF_REBASE
+
+
+def test_rebased_addresses_stay_in_the_array():
+    """Variant 5's shared accesses -- the model's store and load addresses of
+    the second buffer at array origin 0, plus REBASE -- lie inside each
+    kernel's array (24 KB and 32 KB) as it really sits, from REBASE on: the
+    rebased build touches only its own array.  (The first buffer's addresses
+    are the second's without the XOR, inside the same bounds by the same
+    terms; the epilogue's addresses are not XOR-ed, so the rebase cancels.)"""
+    for kernel, size in ((mismatches_128x128x8, 24576), (mismatches_128x256x8, 32768)):
+        rec = []
+        assert kernel(0, 16384, rec) == 0
+        assert rec
+        for addr, nbytes in rec:
+            assert REBASE <= addr + REBASE and addr + REBASE + nbytes <= REBASE + size
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("m,n,k,alpha,beta", [
+    (300, 300, 300, 1.5, 0.5),
+    (1024, 1024, 1024, 1.0, 0.0),   # the smallest plain benchmark config
+    (1000, 777, 263, 1.5, 0.5),     # ragged: edge masks and a k remainder
+    (2500, 2500, 9, 1.5, 0.5),      # the largest sgemm_128x128x8 dispatch, two k blocks
+    (2600, 640, 1000, 1.5, 0.5),    # sgemm_128x256x8 dispatch, unchanged by the rebase
+])
+def test_rebased_build_matches_the_oracle(m, n, k, alpha, beta):
+    """The rebased build of the unmodified reference kernels equals the oracle
+    bit for bit, where the stock build of sgemm_128x128x8 does not: the
+    alignment of the shared array is the whole defect."""
+    import torch
+
+    A = oracle.fill(m, k, 7, 1, 0)
+    B = oracle.fill(k, n, 7, 2, 0)
+    C = oracle.fill(m, n, 7, 3, 0)
+    want = oracle.sgemm_basic(A, B, C, alpha, beta, basic=False)
+    dA, dB = torch.from_numpy(A).cuda(), torch.from_numpy(B).cuda()
+    # the premise: both kernels' array starts REBASE bytes past a 16 KB boundary
+    assert oracle.ref_rebased_premise()
+    rebased = torch.from_numpy(C).cuda()
+    stock = torch.from_numpy(C).cuda()
+    oracle.ref_sgemm_variant(5, dA, dB, rebased, alpha, beta)
+    oracle.ref_sgemm(dA, dB, stock, alpha, beta)
+    torch.cuda.synchronize()
+    assert np.array_equal(rebased.cpu().numpy().view(np.uint32), want.view(np.uint32))
+    if oracle.ref().ref_sgemm_kernel_choice(m, n) == 0 and k >= 64:
+        assert not np.array_equal(stock.cpu().numpy(), want)
+    if oracle.ref().ref_sgemm_kernel_choice(m, n) == 1:
+        assert np.array_equal(stock.cpu().numpy().view(np.uint32), want.view(np.uint32))
