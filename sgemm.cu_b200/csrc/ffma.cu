@@ -39,6 +39,12 @@ using W1 = Cfg<128, 64, 4, 2, 4, 4, kLoaderTma, 2>;        // 8 warps,  96 KB
 // barrier in the main loop).
 using P0 = Cfg<128, 64, 4, 1, 8, 3, kLoaderTma, 3, 8, 1>;  // 4+1 warps, 72 KB
 using P1 = Cfg<128, 64, 4, 1, 8, 4, kLoaderTma, 2, 8, 1>;  // 4+1 warps, 96 KB
+// A 28 x 256 tile of four warps side by side, 7 x 8 outputs per thread, with a
+// producer warp: a 1024 x 1024 output is 37 x 4 = 148 tiles, one per SM, each
+// thread doing 56 FMAs per k step where the 128 x 64 tile (128 tiles, 20 SMs
+// idle) does 64.  One CTA per SM (145 / 217 KB of shared memory).
+using T0 = Cfg<28, 256, 1, 4, 8, 4, kLoaderTma, 1, 8, 1, 7>;  // 4+1 warps, 145 KB
+using T1 = Cfg<28, 256, 1, 4, 8, 6, kLoaderTma, 1, 8, 1, 7>;  // 4+1 warps, 217 KB
 
 struct ConfigDesc {
     const char* name;
@@ -73,7 +79,12 @@ constexpr ConfigDesc describe(const char* name, float eff, float lone = 0.0f) {
 // gives the 4-stage producer tile its measured lone-CTA throughput (1.045 of
 // the 3-stage tile's) and a full-wave figure that keeps multi-wave problems
 // on the tiles that measured best there: at 2048^3 its two CTAs per SM fit the
-// 512 tiles in two waves, yet the 64 x 64 tile is 1.6-2.2% faster.
+// 512 tiles in two waves, yet the 64 x 64 tile is 1.6-2.2% faster.  The
+// 28 x 256 tiles (one CTA per SM, so every wave is "lone") were measured the
+// same way at 768..4096: the 4-stage one is 9-11% faster than the previous
+// pick at 1000^3 and 1024^3 and 8-9% at 896^3 (both betas), 4% slower at
+// 2048^3 with beta = 0.5 and 10-30% slower at 768^3, 1536^3 and from 3072^3
+// up; 0.80 reproduces those picks (the 6-stage one is 1-3% slower still).
 static const ConfigDesc kConfigs[] = {
     describe<C0>("tma_128x256_w8_t8x16_s4", 0.840f),   describe<C1>("tma_128x128_w8_t8x8_s3", 0.900f),
     describe<C2>("tma_128x128_w4_t8x16_s3", 0.875f),   describe<C3>("tma_64x128_w4_t8x8_s4", 0.920f),
@@ -84,6 +95,7 @@ static const ConfigDesc kConfigs[] = {
     describe<C12>("cpa_64x64_w2_t8x8_s4", 0.630f),     describe<C14>("cpa_128x64_w4_t8x8_s3", 0.890f),
     describe<W0>("tma_128x64_w8_t8x4_s3", 0.850f),     describe<W1>("tma_128x64_w8_t8x4_s4", 0.900f),
     describe<P0>("tma_128x64_w4p_t8x8_s3", 0.900f),    describe<P1>("tma_128x64_w4p_t8x8_s4", 0.900f, 1.045f),
+    describe<T0>("tma_28x256_w4p_t7x8_s4", 0.800f),    describe<T1>("tma_28x256_w4p_t7x8_s6", 0.780f),
 };
 constexpr int kNumConfigs = sizeof(kConfigs) / sizeof(kConfigs[0]);
 

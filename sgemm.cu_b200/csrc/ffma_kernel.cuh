@@ -20,7 +20,7 @@
 //    conflict-free 128-bit shared load (instead of transposing A in smem);
 //  - B is kept [32][BN]; each 128-bit load is broadcast to the 4 lanes that
 //    share a column group (warp-level operand broadcast);
-//  - thread tile 8 (m) x TN (n); lanes 4 (m) x 8 (n); warps WM x WN;
+//  - thread tile TM (m, 8 or 7) x TN (n); lanes 4 (m) x 8 (n); warps WM x WN;
 //  - the FMAs are packed (fma.rn.f32x2, two columns of a row per
 //    instruction): the FP32 pipe, not instruction issue, becomes the limit;
 //  - epilogue straight from registers with float4 stores: for a fixed
@@ -37,7 +37,7 @@ namespace ffma {
 enum Loader { kLoaderTma = 0, kLoaderAsync4 = 1 };
 
 template <int BM_, int BN_, int WM_, int WN_, int TN_, int STAGES_, int LOADER_, int MINB_ = 1,
-          int K4U_ = 8, int PRODUCER_ = 0>
+          int K4U_ = 8, int PRODUCER_ = 0, int TM_ = 8>
 struct Cfg {
     static constexpr int BM = BM_, BN = BN_, WM = WM_, WN = WN_, TN = TN_, STAGES = STAGES_;
     static constexpr int LOADER = LOADER_;
@@ -47,16 +47,23 @@ struct Cfg {
     // each stage through a per-stage "empty" mbarrier instead of a CTA barrier.
     static constexpr int PRODUCER = PRODUCER_;
     static constexpr int BK = 32;  // one 128-byte row of A per k block
-    static constexpr int TM = 8;
+    // rows per thread: 8, or 7 for the tile whose 28 rows split a 1024-row
+    // problem into one CTA per SM
+    static constexpr int TM = TM_;
+    static constexpr int WROWS = 4 * TM;  // rows of a warp's tile (4 lanes x TM)
     static constexpr int COMPUTE_THREADS = 32 * WM * WN;
     static constexpr int THREADS = COMPUTE_THREADS + (PRODUCER ? 32 : 0);
     static_assert(!PRODUCER || LOADER_ == 0, "the producer warp issues TMA loads");
-    static_assert(BM == WM * 4 * TM, "4 lanes x 8 rows per warp along m");
+    static_assert(BM == WM * WROWS, "4 lanes x TM rows per warp along m");
     static_assert(BN == WN * 8 * TN, "8 lanes x TN columns per warp along n");
     static_assert(TN % 4 == 0, "columns come in float4 groups");
-    static constexpr int A_BYTES = BM * BK * 4;
+    static constexpr int A_TX = BM * BK * 4;  // bytes one A box brings
+    // A's region in a stage, rounded up to the 1024-byte swizzle atom so that
+    // B (and the next stage) start on one
+    static constexpr int A_BYTES = (A_TX + 1023) / 1024 * 1024;
     static constexpr int B_BYTES = BK * BN * 4;
-    static constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
+    static constexpr int STAGE_BYTES = A_BYTES + B_BYTES;  // stride between stages
+    static constexpr int STAGE_TX = A_TX + B_BYTES;        // bytes a stage's copies bring
     static_assert(A_BYTES % 1024 == 0 && STAGE_BYTES % 1024 == 0, "1024-byte swizzle atoms");
     static constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024;  // + alignment slack
 };
@@ -86,6 +93,19 @@ __device__ __forceinline__ void tile_coords(int bid, int tiles_m, int tiles_n, i
     const int r = bid % per_group;
     tm = first + r % gsz;
     tn = r / gsz;
+}
+
+// A's shared-memory coordinates for a thread: its first row of the tile is
+// r0 = wm * WROWS + lm and its i-th row r0 + 4i, at byte r0 * 128 + i * 512.
+// The 128-byte swizzle XORs a row's 16-byte chunk index with row % 8, which
+// along i alternates between xa0 (even i) and xa1 (odd i).
+template <class C>
+__device__ __forceinline__ void a_coords(int wm, int lm, uint32_t& a_base, uint32_t& xa0,
+                                         uint32_t& xa1) {
+    const int r0 = wm * C::WROWS + lm;
+    a_base = static_cast<uint32_t>(r0 * 128);
+    xa0 = static_cast<uint32_t>(r0 & 7) << 4;
+    xa1 = static_cast<uint32_t>((r0 + 4) & 7) << 4;
 }
 
 // Fragment loads of one k block: A rows for the 4-deep step k4 (4 k-values of
@@ -206,15 +226,15 @@ __device__ __forceinline__ void load_stage_async4(const Operands& p, uint8_t* As
     }
 }
 
-// Thread (wm, wn, lm, ln) owns rows m0 + 32wm + lm + 4i (i < 8) and the float4
-// column groups n0 + wn*8*TN + 4ln + 32g (g < TN/4).
+// Thread (wm, wn, lm, ln) owns rows m0 + WROWS wm + lm + 4i (i < TM) and the
+// float4 column groups n0 + wn*8*TN + 4ln + 32g (g < TN/4).
 template <class C>
 __device__ __forceinline__ void epilogue(const Operands& p, int m0, int n0, int wm, int wn, int lm,
                                          int ln, const float (&acc)[C::TM][C::TN]) {
     const int col0 = n0 + wn * 8 * C::TN + ln * 4;
 #pragma unroll
     for (int i = 0; i < C::TM; ++i) {
-        const int row = m0 + wm * 32 + lm + 4 * i;
+        const int row = m0 + wm * C::WROWS + lm + 4 * i;
         if (row >= p.m) continue;
         float* crow = p.C + (int64_t)row * p.ldc;
 #pragma unroll
@@ -250,7 +270,7 @@ __device__ __forceinline__ void epilogue(const Operands& p, int m0, int n0, int 
 // Epilogue for C rows that are not 16-byte aligned (ldc % 4 != 0 or an
 // unaligned base), where float4 accesses are impossible and per-thread
 // scalar accesses would touch 4 rows x 4 sectors per warp instruction for
-// 128 useful bytes.  Each warp first parks its 32 x (8 TN) outputs in shared
+// 128 useful bytes.  Each warp first parks its WROWS x (8 TN) outputs in shared
 // memory (the stage ring, free once the main loop is done), then walks its
 // rows with consecutive lanes on consecutive columns: one 128-byte row
 // segment per instruction.  The arithmetic per element is the epilogue's
@@ -262,9 +282,9 @@ __device__ __forceinline__ void epilogue_staged(const Operands& p, int m0, int n
                                                 const float (&acc)[C::TM][C::TN], uint8_t* smem) {
     constexpr int W = 8 * C::TN;  // columns of a warp's tile
     constexpr int LD = W + 8;     // row pitch: 8 banks between rows, conflict-free float4 stores
-    static_assert((C::COMPUTE_THREADS / 32) * 32 * LD * 4 <= C::STAGES * C::STAGE_BYTES,
+    static_assert((C::COMPUTE_THREADS / 32) * C::WROWS * LD * 4 <= C::STAGES * C::STAGE_BYTES,
                   "the staged tile fits in the stage ring");
-    float* buf = reinterpret_cast<float*>(smem) + warp * 32 * LD;
+    float* buf = reinterpret_cast<float*>(smem) + warp * C::WROWS * LD;
 #pragma unroll
     for (int i = 0; i < C::TM; ++i)
 #pragma unroll
@@ -273,8 +293,8 @@ __device__ __forceinline__ void epilogue_staged(const Operands& p, int m0, int n
                 make_float4(acc[i][4 * g], acc[i][4 * g + 1], acc[i][4 * g + 2], acc[i][4 * g + 3]);
     __syncwarp();
     const int col0 = n0 + wn * W;
-    for (int r = 0; r < 32; ++r) {
-        const int row = m0 + wm * 32 + r;
+    for (int r = 0; r < C::WROWS; ++r) {
+        const int row = m0 + wm * C::WROWS + r;
         if (row >= p.m) break;
         float* crow = p.C + (int64_t)row * p.ldc;
 #pragma unroll
@@ -358,7 +378,7 @@ __global__ void __launch_bounds__(C::THREADS, C::MINB)
                         break;
                     }
                     uint8_t* st = smem + s * C::STAGE_BYTES;
-                    mbar_arrive_expect_tx(&full_bar[s], C::STAGE_BYTES);
+                    mbar_arrive_expect_tx(&full_bar[s], C::STAGE_TX);
                     tma_load_2d(st, &tmA, &full_bar[s], kb * C::BK, tm * C::BM);
                     tma_load_2d(st + C::A_BYTES, &tmB, &full_bar[s], tn * C::BN, kb * C::BK);
                 }
@@ -373,9 +393,8 @@ __global__ void __launch_bounds__(C::THREADS, C::MINB)
         int lm, ln;
         lane_coords(lane, lm, ln);
         const int m0 = tm * C::BM, n0 = tn * C::BN;
-        const uint32_t a_base = static_cast<uint32_t>((wm * 32 + lm) * 128);
-        const uint32_t xa0 = static_cast<uint32_t>(lm) << 4;
-        const uint32_t xa1 = static_cast<uint32_t>(lm + 4) << 4;
+        uint32_t a_base, xa0, xa1;
+        a_coords<C>(wm, lm, a_base, xa0, xa1);
         const uint32_t b_base = static_cast<uint32_t>((wn * 8 * C::TN + ln * 4) * 4);
         float acc[C::TM][C::TN];
 #pragma unroll
@@ -407,9 +426,8 @@ __global__ void __launch_bounds__(C::THREADS, C::MINB)
     const int nk = (p.op.k + C::BK - 1) / C::BK;
 
     // Per-thread shared-memory offsets (bytes within a stage).
-    const uint32_t a_base = static_cast<uint32_t>((wm * 32 + lm) * 128);
-    const uint32_t xa0 = static_cast<uint32_t>(lm) << 4;        // row % 8 for even i
-    const uint32_t xa1 = static_cast<uint32_t>(lm + 4) << 4;    // row % 8 for odd i
+    uint32_t a_base, xa0, xa1;
+    a_coords<C>(wm, lm, a_base, xa0, xa1);
     const uint32_t b_base = static_cast<uint32_t>((wn * 8 * C::TN + ln * 4) * 4);
 
     float acc[C::TM][C::TN];
@@ -423,7 +441,7 @@ __global__ void __launch_bounds__(C::THREADS, C::MINB)
         auto issue = [&](int kb) {
             const int s = kb % C::STAGES;
             uint8_t* st = smem + s * C::STAGE_BYTES;
-            mbar_arrive_expect_tx(&full_bar[s], C::STAGE_BYTES);
+            mbar_arrive_expect_tx(&full_bar[s], C::STAGE_TX);
             tma_load_2d(st, &tmA, &full_bar[s], kb * C::BK, m0);
             tma_load_2d(st + C::A_BYTES, &tmB, &full_bar[s], n0, kb * C::BK);
         };

@@ -130,9 +130,8 @@ __device__ __forceinline__ bool run_item(const GParams& gp, const GProblem& pr, 
     const int kb1 = min(nk, kb0 + pr.kbps);
     const int nkb = max(0, kb1 - kb0);
 
-    const uint32_t a_base = static_cast<uint32_t>((wm * 32 + lm) * 128);
-    const uint32_t xa0 = static_cast<uint32_t>(lm) << 4;
-    const uint32_t xa1 = static_cast<uint32_t>(lm + 4) << 4;
+    uint32_t a_base, xa0, xa1;
+    ffma::a_coords<C>(wm, lm, a_base, xa0, xa1);
     const uint32_t b_base = static_cast<uint32_t>((wn * 8 * C::TN + ln * 4) * 4);
 
     float acc[C::TM][C::TN];
@@ -149,7 +148,7 @@ __device__ __forceinline__ bool run_item(const GParams& gp, const GProblem& pr, 
             const uint32_t gs = g + j;
             const int s = gs % S;
             uint8_t* st = smem + s * SLOT_BYTES;
-            mbar_arrive_expect_tx(&full_bar[s], C::STAGE_BYTES);
+            mbar_arrive_expect_tx(&full_bar[s], C::STAGE_TX);
             tma_load_2d(st, tmA, &full_bar[s], (kb0 + j) * C::BK, m0);
             tma_load_2d(st + C::A_BYTES, tmB, &full_bar[s], n0, (kb0 + j) * C::BK);
         };

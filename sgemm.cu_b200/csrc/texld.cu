@@ -118,9 +118,8 @@ __global__ void __launch_bounds__(C::THREADS, C::MINB) texld_gemm_kernel(const P
     ffma::tile_coords(blockIdx.x, p.tiles_m, p.tiles_n, tm, tn);
     const int m0 = tm * C::BM, n0 = tn * C::BN;
     const int nk = (p.op.k + C::BK - 1) / C::BK;
-    const uint32_t a_base = static_cast<uint32_t>((wm * 32 + lm) * 128);
-    const uint32_t xa0 = static_cast<uint32_t>(lm) << 4;
-    const uint32_t xa1 = static_cast<uint32_t>(lm + 4) << 4;
+    uint32_t a_base, xa0, xa1;
+    ffma::a_coords<C>(wm, lm, a_base, xa0, xa1);
     const uint32_t b_base = static_cast<uint32_t>((wn * 8 * C::TN + ln * 4) * 4);
 
     float acc[C::TM][C::TN];

@@ -97,6 +97,22 @@ def test_every_config_bit_exact(cfg, shape):
     _assert_equal(got, oracle.sgemm_basic(A, B, C, 1.5, 0.5, basic=False))
 
 
+@pytest.mark.parametrize("name", ["tma_28x256_w4p_t7x8_s4", "tma_28x256_w4p_t7x8_s6"])
+@pytest.mark.parametrize("m,n,k,ldc,ab", [
+    (1024, 1024, 1024, None, (1.0, 0.0)),   # 37 x 4 tiles, the last row tile 16 rows
+    (1000, 1000, 1000, None, (1.5, 0.5)),   # 36 x 4 tiles, ragged columns
+    (57, 300, 72, 301, (1.5, 0.5)),         # C rows not 16-byte aligned: staged epilogue
+    (28, 256, 8, None, (1.0, 0.0)),         # exactly one tile, one k block
+], ids=["1024", "1000", "ldc_odd", "one_tile"])
+def test_seven_row_thread_tile_bit_exact(name, m, n, k, ldc, ab):
+    # the 28 x 256 tile: 7 rows per thread, so each warp's rows start at a
+    # multiple of 28 and the A swizzle phase follows the row, not the lane
+    cfg = sg.config_names().index(name)
+    A, B, C = _inputs(m, n, k, 9, 0)
+    got = _run_ours(A, B, C, *ab, lds=(None, None, ldc), config=cfg)
+    _assert_equal(got, oracle.sgemm_basic(A, B, C, *ab, basic=False))
+
+
 @pytest.mark.parametrize("lds", [(None, None, None), (36, 52, 60), (33, 49, 51), (37, 48, 50)],
                          ids=["packed", "ld_aligned", "ld_odd", "lda_odd"])
 def test_general_strides_and_canaries(lds):
