@@ -42,9 +42,10 @@ using P1 = Cfg<128, 64, 4, 1, 8, 4, kLoaderTma, 2, 8, 1>;  // 4+1 warps, 96 KB
 // A 28 x 256 tile of four warps side by side, 7 x 8 outputs per thread, with a
 // producer warp: a 1024 x 1024 output is 37 x 4 = 148 tiles, one per SM, each
 // thread doing 56 FMAs per k step where the 128 x 64 tile (128 tiles, 20 SMs
-// idle) does 64.  One CTA per SM (145 / 217 KB of shared memory).
-using T0 = Cfg<28, 256, 1, 4, 8, 4, kLoaderTma, 1, 8, 1, 7>;  // 4+1 warps, 145 KB
-using T1 = Cfg<28, 256, 1, 4, 8, 6, kLoaderTma, 1, 8, 1, 7>;  // 4+1 warps, 217 KB
+// idle) does 64.  With 4 stages one CTA fits an SM; with 3, two do (2048^3:
+// 592 tiles, two full waves of eight compute warps per SM).
+using T0 = Cfg<28, 256, 1, 4, 8, 4, kLoaderTma, 1, 8, 1, 7>;  // 4+1 warps, 145 KB, 1/SM
+using T3 = Cfg<28, 256, 1, 4, 8, 3, kLoaderTma, 2, 8, 1, 7>;  // 4+1 warps, 109 KB, 2/SM
 
 struct ConfigDesc {
     const char* name;
@@ -80,11 +81,17 @@ constexpr ConfigDesc describe(const char* name, float eff, float lone = 0.0f) {
 // the 3-stage tile's) and a full-wave figure that keeps multi-wave problems
 // on the tiles that measured best there: at 2048^3 its two CTAs per SM fit the
 // 512 tiles in two waves, yet the 64 x 64 tile is 1.6-2.2% faster.  The
-// 28 x 256 tiles (one CTA per SM, so every wave is "lone") were measured the
-// same way at 768..4096: the 4-stage one is 9-11% faster than the previous
-// pick at 1000^3 and 1024^3 and 8-9% at 896^3 (both betas), 4% slower at
-// 2048^3 with beta = 0.5 and 10-30% slower at 768^3, 1536^3 and from 3072^3
-// up; 0.80 reproduces those picks (the 6-stage one is 1-3% slower still).
+// 28 x 256 tiles were measured the same way at 768..12288.  The 4-stage one
+// (one CTA per SM) is 9-11% faster than the previous pick at 1000^3 and
+// 1024^3 and 8-9% at 896^3 (both betas) and slower elsewhere; 0.80
+// reproduces those picks.  The 3-stage one (two CTAs per SM) is 10-12%
+// faster at 2048^3, 1.4-1.9% at 3072^3 and 6144^3, within 0.5% at 4096^3,
+// 8192^3 and 12288^3, 3% slower at 1280^3 and 2560^3 and far slower at
+// 1536^3 (330 tiles: a third, near-empty wave); 0.99 picks it at 2048^3,
+// 4096^3 and 6144^3 and leaves 8192^3 on the 128 x 64 tile, and its lone
+// figure, 0.95, keeps 896..1024 on the 4-stage tile, 1-3% faster there.
+// (Measured and dropped: 6 stages, 1-3% slower than 4; eight 7 x 4-thread
+// warps, 2-5% slower at beta = 0; 32-row rasterisation bands, no change.)
 static const ConfigDesc kConfigs[] = {
     describe<C0>("tma_128x256_w8_t8x16_s4", 0.840f),   describe<C1>("tma_128x128_w8_t8x8_s3", 0.900f),
     describe<C2>("tma_128x128_w4_t8x16_s3", 0.875f),   describe<C3>("tma_64x128_w4_t8x8_s4", 0.920f),
@@ -95,7 +102,7 @@ static const ConfigDesc kConfigs[] = {
     describe<C12>("cpa_64x64_w2_t8x8_s4", 0.630f),     describe<C14>("cpa_128x64_w4_t8x8_s3", 0.890f),
     describe<W0>("tma_128x64_w8_t8x4_s3", 0.850f),     describe<W1>("tma_128x64_w8_t8x4_s4", 0.900f),
     describe<P0>("tma_128x64_w4p_t8x8_s3", 0.900f),    describe<P1>("tma_128x64_w4p_t8x8_s4", 0.900f, 1.045f),
-    describe<T0>("tma_28x256_w4p_t7x8_s4", 0.800f),    describe<T1>("tma_28x256_w4p_t7x8_s6", 0.780f),
+    describe<T0>("tma_28x256_w4p_t7x8_s4", 0.800f),    describe<T3>("tma_28x256_w4p_t7x8_s3", 0.990f, 0.950f),
 };
 constexpr int kNumConfigs = sizeof(kConfigs) / sizeof(kConfigs[0]);
 
