@@ -113,6 +113,21 @@ def test_seven_row_thread_tile_bit_exact(name, m, n, k, ldc, ab):
     _assert_equal(got, oracle.sgemm_basic(A, B, C, *ab, basic=False))
 
 
+@pytest.mark.parametrize("size,beta,want", [
+    (1024, 0.0, "tma_28x256_w4p_t7x8_s4"),
+    (1024, 0.5, "tma_28x256_w4p_t7x8_s4"),
+    (1000, 0.5, "tma_28x256_w4p_t7x8_s4"),
+    (2048, 0.5, "tma_28x256_w4p_t7x8_s3"),
+    (8192, 0.5, "tma_128x64_w4_t8x8_s3"),
+])
+def test_dispatch_picks_the_measured_fastest_tile(size, beta, want):
+    # the cost model's choice at sizes where every configuration was timed
+    # against the others on a B200: a change to the model (or to a tile's
+    # shared memory or registers, which set its CTAs per SM) that moves one of
+    # these sizes off its fastest tile fails here
+    assert sg.config_names()[sg.select_config(size, size, size, beta=beta)] == want
+
+
 @pytest.mark.parametrize("lds", [(None, None, None), (36, 52, 60), (33, 49, 51), (37, 48, 50)],
                          ids=["packed", "ld_aligned", "ld_odd", "lda_odd"])
 def test_general_strides_and_canaries(lds):
