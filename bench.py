@@ -882,7 +882,7 @@ def run(args):
         torch.cuda.empty_cache()
     if rank == 0 and world == 1 and not args.skip_serving:
         try:
-            result["serving"] = _serving_leg(sg, [500.0, 1000.0, 2000.0, 4000.0, 8000.0],
+            result["serving"] = _serving_leg(sg, [500.0, 1000.0, 2000.0, 4000.0, 8000.0, 16000.0],
                                              args.serving_requests,
                                              sms * 256 * sm_max * 1e-3,
                                              peaks["bf16_tflops"] * 1e3 / 6, peaks["hbm_gbs"])

@@ -9,6 +9,8 @@
 // the reference kernel's bit for bit.  Like the reference it always reads C.
 //
 // Also here: the bounded-wait self-test (sgemm_b200_selftest_wait_timeout).
+#include <algorithm>
+
 #include "common.h"
 #include "ptx.cuh"
 #include "rng.h"
@@ -26,14 +28,31 @@ __global__ void basic_kernel(int m, int n, int k, float alpha, const float* __re
     C[(int64_t)y * ldc + x] = fmaf(acc, alpha, __fmul_rn(c, beta));
 }
 
+// Element (r, c) gets rng_value(key, r * cols + c): the value depends only on
+// the seed, the tag and that flat index, whatever the row pitch.  Rows run
+// along the grid's y, each thread makes 4 consecutive columns per step, and
+// when rows start 16-byte aligned (vec) a step is one float4 store -- a
+// bandwidth-bound write instead of a 64-bit division and a scalar store per
+// element.
 __global__ void fill_kernel(float* X, int rows, int cols, int ld, uint64_t seed, uint32_t tag,
-                            int dist) {
-    const int64_t total = (int64_t)rows * cols;
+                            int dist, int vec) {
     const uint64_t key = rng_key(seed, tag);
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
-         i += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t r = i / cols, c = i % cols;
-        X[r * ld + c] = rng_value(key, static_cast<uint64_t>(i), dist);
+    for (int r = blockIdx.y; r < rows; r += gridDim.y) {
+        float* row = X + (int64_t)r * ld;
+        const uint64_t base = (uint64_t)r * (uint64_t)cols;
+        for (int c = 4 * (blockIdx.x * blockDim.x + threadIdx.x); c < cols;
+             c += 4 * gridDim.x * blockDim.x) {
+            float v[4];
+#pragma unroll
+            for (int e = 0; e < 4; ++e) v[e] = rng_value(key, base + (uint64_t)(c + e), dist);
+            if (vec && c + 3 < cols) {
+                *reinterpret_cast<float4*>(row + c) = make_float4(v[0], v[1], v[2], v[3]);
+            } else {
+#pragma unroll
+                for (int e = 0; e < 4; ++e)
+                    if (c + e < cols) row[c + e] = v[e];
+            }
+        }
     }
 }
 
@@ -100,12 +119,12 @@ extern "C" int sgemm_b200_fill_random(float* X, int rows, int cols, int ld, uint
     }
     if (rows == 0 || cols == 0) return SGEMM_B200_OK;
     if (!X) return SGEMM_B200_ERR_INVALID_ARG;
-    const int64_t total = (int64_t)rows * cols;
     const int threads = 256;
-    int64_t blocks = (total + threads - 1) / threads;
-    if (blocks > 148 * 64) blocks = 148 * 64;
-    sgb::fill_kernel<<<(int)blocks, threads, 0, sgb::as_stream(stream)>>>(X, rows, cols, ld, seed,
-                                                                          tag, dist);
+    const int vec = (ld % 4 == 0) && (reinterpret_cast<uintptr_t>(X) % 16 == 0);
+    const dim3 grid(std::min((cols + 4 * threads - 1) / (4 * threads), 1024),
+                    std::min(rows, 65535));
+    sgb::fill_kernel<<<grid, threads, 0, sgb::as_stream(stream)>>>(X, rows, cols, ld, seed, tag,
+                                                                   dist, vec);
     int s = sgb::cuda_status(cudaGetLastError());
     sgb::set_last_status(s);
     return s;

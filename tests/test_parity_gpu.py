@@ -238,14 +238,22 @@ def test_reference_naive_kernel_matches_ours():
     assert torch.equal(c1, c2)
 
 
-def test_device_fill_matches_host_generator():
+@pytest.mark.parametrize("rows,cols,ld", [(33, 129, 129), (40, 256, 256), (33, 129, 132),
+                                          (3, 5000, 5003), (70000, 3, 4)],
+                         ids=["odd_rows", "aligned", "aligned_pitch_ragged", "wide", "tall"])
+def test_device_fill_matches_host_generator(rows, cols, ld):
+    # every element's value depends only on (seed, tag, row * cols + col):
+    # scalar and float4 stores, any pitch, more rows than one grid dimension
     torch = _torch()
     for dist in (0, 1, 2):
-        X = torch.empty((33, 129), device="cuda")
+        big = torch.full((rows, ld), float("nan"), device="cuda")
+        X = big[:, :cols]
         sg.fill_random(X, 99, 4, dist)
         torch.cuda.synchronize()
-        want = oracle.fill(33, 129, 99, 4, dist)
-        assert np.array_equal(X.cpu().numpy().view(np.uint32), want.view(np.uint32))
+        want = oracle.fill(rows, cols, 99, 4, dist)
+        got = big.cpu().numpy()
+        assert np.array_equal(got[:, :cols].view(np.uint32), want.view(np.uint32))
+        assert np.isnan(got[:, cols:]).all()
 
 
 @pytest.mark.parametrize("size", [4096, 8192])
