@@ -671,6 +671,35 @@ def _pct(xs, q):
     return xs[min(len(xs) - 1, max(0, int(np.ceil(q * len(xs))) - 1))]
 
 
+def _serving_kernel_ceiling(sg, n_batches=4, batch=32, reps=5):
+    """The plain server's device ceiling on its own mix: the grouped FFMA kernel
+    alone, one launch at a time, on batches of serving-mix shapes whose
+    operands were filled beforehand (untimed) -- no queueing, no operand
+    generation, no second batch in flight."""
+    import torch
+    shapes, _ = sg.serving_workload(n_batches * batch, 8000.0, 11)
+    flush = torch.empty((256 << 20) // 4, device="cuda")
+    flops, ms = 0.0, 0.0
+    for b in range(n_batches):
+        part = shapes[b * batch:(b + 1) * batch]
+        specs = []
+        for i, (m, n, k) in enumerate(part):
+            X = [torch.empty((r, c), device="cuda") for r, c in ((m, k), (k, n), (m, n))]
+            for tag, T in zip((1, 2, 3), X):
+                sg.fill_random(T, 11 + b * batch + i, tag, sg.DIST_UNIFORM_PM1)
+            specs.append((X[0], X[1], X[2], 1.0, 0.5))
+        plan = sg.GroupedPlan(specs)
+        t = _time_steps(torch, plan.launch, reps, 3, flush)
+        plan.close()
+        del specs
+        flops += sum(2.0 * m * n * k for (m, n, k) in part)
+        ms += statistics.median(t)
+    torch.cuda.empty_cache()
+    return {"tflops": round(flops / (ms * 1e-3) * 1e-12, 2), "batches": n_batches,
+            "batch_size": batch, "gflop": round(flops * 1e-9, 1),
+            "note": "grouped FFMA kernel alone, one graph launch per batch, operands resident"}
+
+
 def _serving_leg(sg, rates, n_requests, simt_gflops, tc_useful_gflops, hbm_gbs):
     out = {"workload": "Poisson arrivals; 60% M~U[16,256] N=K=4096, 40% M=N=K log-uniform "
                        "[512,4096]; operands generated and resident on the device; 64 GB "
@@ -712,6 +741,10 @@ def _serving_leg(sg, rates, n_requests, simt_gflops, tc_useful_gflops, hbm_gbs):
                 "achieved_over_roofline": round(st["gflops"] / roof, 4),
                 "saturated": bool(st["gflops"] < 0.97 * offered)})
         srv.close()
+    try:
+        out["plain_kernel_ceiling"] = _serving_kernel_ceiling(sg)
+    except Exception as e:  # a measurement aid: never lose the leg's runs to it
+        out["plain_kernel_ceiling"] = {"error": f"{type(e).__name__}: {e}"}
     out["bound_note"] = ("slowdown = a request's latency (submit to completion) / its shape's "
                          "device time served alone through the same server path (isolated); "
                          "achieved_over_roofline = achieved GFLOP/s / the mix's roofline (each "
