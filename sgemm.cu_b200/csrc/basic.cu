@@ -29,8 +29,9 @@ __global__ void basic_kernel(int m, int n, int k, float alpha, const float* __re
 }
 
 // Element (r, c) gets rng_value(key, r * cols + c): the value depends only on
-// the seed, the tag and that flat index, whatever the row pitch.  Rows run
-// along the grid's y, each thread makes 4 consecutive columns per step, and
+// the seed, the tag and that flat index, whatever the row pitch.  Blocks
+// stride over rows along the grid's y, each thread makes 4 consecutive
+// columns per step, and
 // when rows start 16-byte aligned (vec) a step is one float4 store -- a
 // bandwidth-bound write instead of a 64-bit division and a scalar store per
 // element.
@@ -121,8 +122,12 @@ extern "C" int sgemm_b200_fill_random(float* X, int rows, int cols, int ld, uint
     if (!X) return SGEMM_B200_ERR_INVALID_ARG;
     const int threads = 256;
     const int vec = (ld % 4 == 0) && (reinterpret_cast<uintptr_t>(X) % 16 == 0);
-    const dim3 grid(std::min((cols + 4 * threads - 1) / (4 * threads), 1024),
-                    std::min(rows, 65535));
+    // about 16 blocks per SM in all, each striding over rows: long-lived
+    // blocks instead of one short block per 1024-column row slab
+    const int gx = std::min((cols + 4 * threads - 1) / (4 * threads), 1024);
+    const int sms = sgb::device_info().sm_count > 0 ? sgb::device_info().sm_count : 148;
+    const int gy = std::min({rows, 65535, std::max(1, (sms * 16 + gx - 1) / gx)});
+    const dim3 grid(gx, gy);
     sgb::fill_kernel<<<grid, threads, 0, sgb::as_stream(stream)>>>(X, rows, cols, ld, seed, tag,
                                                                    dist, vec);
     int s = sgb::cuda_status(cudaGetLastError());
