@@ -150,6 +150,22 @@ def test_pack_path_matches_the_oracle(m, n, k, pads):
     _assert_equal(got, oracle.sgemm_basic(A, B, C, 1.5, 0.5, basic=False))
 
 
+@pytest.mark.parametrize("m,n,k,pads,tile", [
+    (1001, 1001, 1001, (1, 1, 1), "tma_28x256_w4p_t7x8_s4"),
+    (2049, 2047, 1999, (3, 1, 1), "tma_28x256_w4p_t7x8_s3"),
+], ids=["1001_both_packed", "2049_a_packed"])
+def test_pack_path_on_the_28_row_tiles(m, n, k, pads, tile):
+    # unaligned strides at the sizes where the dispatcher picks a 28 x 256
+    # tile: the operands are packed to aligned rows, that tile runs, and the
+    # result is the oracle's bit for bit
+    lds = (k + pads[0], n + pads[1], n + pads[2])
+    assert sg.config_names()[sg.select_config(m, n, k, None, lds[0], None, lds[1],
+                                              beta=0.5)] == tile
+    A, B, C = _inputs(m, n, k, 29, 0)
+    got = _run_ours(A, B, C, 1.5, 0.5, lds=lds)
+    _assert_equal(got, oracle.sgemm_basic(A, B, C, 1.5, 0.5, basic=False))
+
+
 def test_beta_zero_never_reads_c():
     m, n, k = 140, 260, 40
     A, B, _ = _inputs(m, n, k, 4, 0)
