@@ -449,11 +449,16 @@ __device__ __forceinline__ void split_bt_tile(const float* __restrict__ B, int k
     }
 }
 
+// Blocks loop over the 64 x 64 tiles (about 8 per SM in all) rather than one
+// short block per tile.
 template <int PATH>
 __global__ void split_bt_kernel(const float* __restrict__ B, int k, int n, int ldb, int kp,
-                                uint8_t* __restrict__ out) {
+                                uint8_t* __restrict__ out, int tiles_n, int tiles) {
     __shared__ float tile[64][65];
-    split_bt_tile<PATH>(B, k, n, ldb, kp, out, blockIdx.x, blockIdx.y, tile);
+    for (int t = blockIdx.x; t < tiles; t += gridDim.x) {
+        split_bt_tile<PATH>(B, k, n, ldb, kp, out, t % tiles_n, t / tiles_n, tile);
+        __syncthreads();  // the next tile's loads overwrite `tile`
+    }
 }
 
 template <int PATH>
@@ -487,8 +492,10 @@ static int launch(int m, int n, int k, float alpha, const float* A, int lda, con
         int64_t blocks = (total + 255) / 256;
         if (blocks > 148 * 32) blocks = 148 * 32;
         split_a_kernel<PATH><<<(int)blocks, 256, 0, stream>>>(A, m, k, lda, kp, wa);
-        dim3 g(div_up(n, 64), div_up(kp, 64));
-        split_bt_kernel<PATH><<<g, 256, 0, stream>>>(B, k, n, ldb, kp, wb);
+        const int tiles_n = div_up(n, 64), tiles = tiles_n * div_up(kp, 64);
+        const int sms = device_info().sm_count > 0 ? device_info().sm_count : 148;
+        split_bt_kernel<PATH><<<std::min(tiles, sms * 8), 256, 0, stream>>>(B, k, n, ldb, kp, wb,
+                                                                             tiles_n, tiles);
     }
 
     const CUtensorMapDataType dt =

@@ -169,3 +169,72 @@ def test_split_error_not_worse_than_plain(dist, size):
         assert results[path]["non_finite"] == 0
         for stat in ("max_rel", "mean_rel", "max_componentwise"):
             assert results[path][stat] <= results["plain"][stat], (path, stat, results)
+
+
+def _bf16_rn(x):
+    """float32 -> nearest bfloat16 (ties to even), as float32 (finite inputs)."""
+    u = np.ascontiguousarray(x, dtype=np.float32).view(np.uint32).astype(np.uint64)
+    r = ((u + 0x7FFF + ((u >> 16) & 1)) >> 16) << 16
+    return r.astype(np.uint32).view(np.float32)
+
+
+def _tf32_rna(x):
+    """float32 -> nearest TF32 (10-bit mantissa), ties away from zero, as the
+    conversion cvt.rna.tf32.f32 rounds (finite inputs)."""
+    u = np.ascontiguousarray(x, dtype=np.float32).view(np.uint32).astype(np.uint64)
+    r = (u + 0x1000) & ~np.uint64(0x1FFF)
+    return r.astype(np.uint32).view(np.float32)
+
+
+def _planes(path, X):
+    """The split of every element of X into the path's planes (float32)."""
+    X = X.astype(np.float32)
+    if path == "bf16x6":
+        h = _bf16_rn(X)
+        r1 = (X - h).astype(np.float32)
+        m = _bf16_rn(r1)
+        r2 = (r1 - m).astype(np.float32)
+        return [h, m, _bf16_rn(r2)]
+    h = _tf32_rna(X)
+    return [h, _tf32_rna((X - h).astype(np.float32))]
+
+
+@pytest.mark.parametrize("path", ["bf16x6", "tf32x3"])
+@pytest.mark.parametrize("m,n,k", [(70, 90, 45), (130, 200, 136), (3, 257, 1)],
+                         ids=["ragged", "multi_tile", "thin"])
+def test_prepass_planes_bit_exact(path, m, n, k):
+    """The pre-pass planes, read back from the caller's workspace, equal a
+    numpy restatement of the split bit for bit: A as [split][m][kp] row-major,
+    B transposed as [split][n][kp], kp = k rounded up to 8, zeros in the
+    padding; BF16x6 stores h, m, l as bfloat16 (each the nearest bfloat16 of
+    the remainder), TF32x3 stores h, l as float32 rounded to TF32."""
+    torch = _torch()
+    A, B, C = (oracle.fill(r, c, 31, t, 2) for r, c, t in ((m, k, 1), (k, n, 2), (m, n, 3)))
+    p = sg.PATHS[path]
+    ws = torch.zeros(sg.split_workspace_size(p, m, n, k) // 4 + 1, dtype=torch.float32,
+                     device="cuda")
+    dA, dB, dC = (torch.from_numpy(x).cuda() for x in (A, B, C))
+    sg.sgemm_split(path, dA, dB, dC, 1.5, 0.5, workspace=ws)
+    torch.cuda.synchronize()
+    raw = ws.cpu().numpy().view(np.uint8)
+    base = (-ws.data_ptr()) % 1024
+    kp = (k + 7) // 8 * 8
+    ns, esz = (3, 2) if path == "bf16x6" else (2, 4)
+    a_bytes = (ns * m * kp * esz + 1023) // 1024 * 1024
+
+    def read(off, rows):
+        blob = raw[base + off: base + off + ns * rows * kp * esz]
+        if esz == 2:
+            v = (blob.view(np.uint16).astype(np.uint32) << 16).view(np.float32)
+        else:
+            v = blob.view(np.float32)
+        return v.reshape(ns, rows, kp)
+
+    got_a, got_b = read(0, m), read(a_bytes, n)
+    Ap = np.zeros((m, kp), np.float32)
+    Ap[:, :k] = A
+    Bt = np.zeros((n, kp), np.float32)
+    Bt[:, :k] = B.T
+    for s, (pa, pb) in enumerate(zip(_planes(path, Ap), _planes(path, Bt))):
+        assert np.array_equal(got_a[s].view(np.uint32), pa.view(np.uint32)), f"A plane {s}"
+        assert np.array_equal(got_b[s].view(np.uint32), pb.view(np.uint32)), f"B plane {s}"
