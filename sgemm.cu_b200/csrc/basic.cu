@@ -31,10 +31,10 @@ __global__ void basic_kernel(int m, int n, int k, float alpha, const float* __re
 // Element (r, c) gets rng_value(key, r * cols + c): the value depends only on
 // the seed, the tag and that flat index, whatever the row pitch.  Blocks
 // stride over rows along the grid's y, each thread makes 4 consecutive
-// columns per step, and
-// when rows start 16-byte aligned (vec) a step is one float4 store -- a
-// bandwidth-bound write instead of a 64-bit division and a scalar store per
-// element.
+// columns per step, and when rows start 16-byte aligned (vec) a step is one
+// float4 store; no 64-bit division per element.  The two 64-bit multiplies of
+// the mixing function per element then bound it (integer throughput), not
+// the stores.
 __global__ void fill_kernel(float* X, int rows, int cols, int ld, uint64_t seed, uint32_t tag,
                             int dist, int vec) {
     const uint64_t key = rng_key(seed, tag);
