@@ -22,6 +22,10 @@ by its own CUDA events with an L2-sized flush write in between steps.
                the whole result checked bit for bit and against FP64
   split_configs  plain / BF16x6 / TF32x3 at 8192^3 and 16384^3 with entries
                sign * 2^e * U[1,2), GFLOP/s and FP64-checked error
+  sweep        the square sweep M=N=K = 1024..16384 in steps of 1024 plus the
+               odd sizes 1000, 3001, 5003 (alpha=1.5, beta=0.5, A, B, C
+               uniform[-1, 1) seed 0): GFLOP/s, fraction of the SIMT peak and
+               the kernel picked per size, sampled rows checked bit for bit
   grouped, serving  the 512-problem grouped launch and the Poisson serving loop
 All FP64 checks run inside the cpu_baseline leg (the oracle is the checker
 there); the other legs only collect sampled output rows.
@@ -30,7 +34,9 @@ there); the other legs only collect sampled output rows.
 this size) built from its sources for sm_100a, same workload and metric, and
 at M=N=K=1024 its 128x128x8 kernel both as built (wrong results on sm_100a)
 and from the rebased test-only build that repairs it, each checked bit for
-bit.  `--ref-build rebased` times that repaired build instead of the stock one
+bit; its sweep leg times the reference's sgemm() over the same sizes (and the
+rebased build where the stock dispatch picks 128x128x8).
+`--ref-build rebased` times that repaired build instead of the stock one
 (a labelled comparison for sizes up to 2500; the default arm stays stock).
 
 Multi-GPU: replicas (the GEMM has no exchange step in this scope); each rank
@@ -54,6 +60,10 @@ sys.path.insert(0, os.path.join(ROOT, "sgemm.cu_b200"))
 SIZE = 8192
 ALPHA, BETA = 1.5, 0.5
 SEED = 0
+# the plain path's square sweep: 1024..16384 in steps of 1024 and the sizes
+# that are not multiples of a tile
+SWEEP_SIZES = sorted([1000, 3001, 5003] + list(range(1024, 16384 + 1, 1024)))
+SWEEP_ROWS = 8  # sampled output rows per size, checked bit for bit in the CPU leg
 
 
 # ------------------------------------------------------------------ helpers --
@@ -488,6 +498,46 @@ def _config_1024_leg(torch, sg, steps, warmup):
     return res, ("config_1024", n, 0, ids, {"plain": out}, (1.0, 0.0), ("plain",))
 
 
+def _sweep_steps(n):
+    """Timed steps per sweep size: more where one GEMM is short."""
+    return 20 if n <= 2048 else (10 if n <= 4096 else 3)
+
+
+def _sweep_leg(torch, sg, sizes, warmup, peak_gflops, l2_bytes):
+    """The plain square sweep: per size, device GFLOP/s (mean of the timed
+    steps, an L2-sized flush between steps), the fraction of the FP32 SIMT
+    peak, the configuration the dispatcher picks and whether a pack step runs,
+    and SWEEP_ROWS output rows of the first GEMM for the cpu_baseline leg's
+    bit-for-bit check."""
+    flush = torch.empty(int(l2_bytes) // 4, device="cuda")
+    out, checks = {}, []
+    for n in sizes:
+        A = torch.empty((n, n), device="cuda")
+        B = torch.empty_like(A)
+        C = torch.empty_like(A)
+        sg.fill_random(A, SEED, 1, sg.DIST_UNIFORM_PM1)
+        sg.fill_random(B, SEED, 2, sg.DIST_UNIFORM_PM1)
+        sg.fill_random(C, SEED, 3, sg.DIST_UNIFORM_PM1)
+        ids = np.linspace(0, n - 1, SWEEP_ROWS).astype(np.int32)
+        sg.sgemm(A, B, C, ALPHA, BETA)
+        torch.cuda.synchronize()
+        rows = C[torch.from_numpy(ids).long().cuda()].cpu().numpy()
+        ms = _time_steps(torch, lambda: sg.sgemm(A, B, C, ALPHA, BETA), _sweep_steps(n), warmup,
+                         flush)
+        t = statistics.mean(ms)
+        g = 2.0 * n ** 3 / (t * 1e-3) * 1e-9
+        out[str(n)] = {"gflops": round(g, 1), "frac_of_simt_peak": round(g / peak_gflops, 4),
+                       "ms_per_step": round(t, 4), "steps": len(ms),
+                       "kernel_config": sg.config_names()[sg.select_config(n, n, n, A, n, B, n,
+                                                                           beta=BETA)],
+                       "packed": bool(sg.packs(n, n, n, A, n, B, n)), "check": None}
+        checks.append((f"sweep_{n}", n, 0, ids, {"plain": rows}, (ALPHA, BETA), ("plain",)))
+        del A, B, C
+    del flush
+    torch.cuda.empty_cache()
+    return out, checks
+
+
 def _split_configs_leg(torch, sg, sizes, steps, n_rows=32):
     """The split-precision config: M=N=K in `sizes`, entries sign * 2^e * U[1,2)
     with e uniform in [-10, 10]; plain, BF16x6 and TF32x3 GFLOP/s, and sampled
@@ -871,6 +921,14 @@ def run(args):
     if rank == 0 and world == 1:
         result["config_1024"], chk = _config_1024_leg(torch, sg, max(20, args.steps), args.warmup)
         checks.append(chk)
+    if rank == 0 and world == 1 and not args.skip_sweep:
+        result["sweep"], more = _sweep_leg(torch, sg, SWEEP_SIZES, args.warmup, peak_max,
+                                           peaks.get("l2_bytes", 126 << 20))
+        result["sweep_note"] = ("M=N=K, alpha=1.5, beta=0.5, A, B, C uniform[-1,1) seed 0; "
+                                "GFLOP/s over the timed steps' mean; frac of the FP32 SIMT "
+                                "peak at the max clock; check: sampled rows against the "
+                                "oracle, bit for bit")
+        checks += more
     split_rows = np.linspace(0, SIZE - 1, 64).astype(np.int32)
     if rank == 0 and world == 1 and not args.skip_library:
         result["library"] = _library_leg(torch, A, B, C0, flush, max(10, args.steps // 2))
@@ -900,6 +958,11 @@ def run(args):
             result["split"]["plain_error_vs_fp64_same_rows"] = uni["plain"]
         if "config_1024" in errors and "config_1024" in result:
             result["config_1024"]["check"] = errors["config_1024"]["plain"]
+        for key, row in result.get("sweep", {}).items():
+            e = errors.get(f"sweep_{key}", {}).get("plain")
+            if e:
+                row["check"] = {"bit_exact": e["bit_exact"], "elements": e["elements"],
+                                "max_rel_vs_fp64": e["max_rel"]}
         for label, errs in errors.items():
             if label.startswith("pow2_"):
                 for name, e in errs.items():
@@ -1028,7 +1091,62 @@ def run_reference(args, torch, peaks, sms, local):
                                                            args.warmup)
         except Exception as e:
             result["config_1024"] = {"error": f"{type(e).__name__}: {e}"}
+    if not rebased and not args.skip_sweep:
+        del A, B, C
+        torch.cuda.empty_cache()
+        try:
+            result["sweep"] = _reference_sweep(torch, oracle, SWEEP_SIZES, args.warmup, peak,
+                                               flush)
+            result["sweep_note"] = ("the reference's sgemm() over the library arm's sweep "
+                                    "sizes and inputs; where its dispatch picks 128x128x8 the "
+                                    "rebased test-only build is timed beside the stock one; "
+                                    "check: sampled rows against the oracle, bit for bit")
+        except Exception as e:
+            result["sweep"] = {"error": f"{type(e).__name__}: {e}"}
     print(json.dumps(result))
+
+
+def _reference_sweep(torch, oracle, sizes, warmup, peak_gflops, flush):
+    """The reference's sgemm() on the sweep sizes: the same seeded inputs
+    (from the oracle's host generator), the same timing as the library arm's
+    sweep leg, and SWEEP_ROWS rows of the first GEMM checked bit for bit
+    against the oracle.  Where the reference dispatches sgemm_128x128x8, whose
+    stock sm_100a build returns wrong values, the rebased test-only build is
+    timed beside it, so a correct reference number exists at every size."""
+    rebase_ok = oracle.ref_rebased_premise()
+    out = {}
+    for n in sizes:
+        hA = oracle.fill(n, n, SEED, 1, 0)
+        hB = oracle.fill(n, n, SEED, 2, 0)
+        hC = oracle.fill(n, n, SEED, 3, 0)
+        ids = np.linspace(0, n - 1, SWEEP_ROWS).astype(np.int32)
+        want = oracle.sgemm_basic(hA[ids], hB, hC[ids], ALPHA, BETA, basic=False)
+        A, B = torch.from_numpy(hA).cuda(), torch.from_numpy(hB).cuda()
+        del hA, hB
+        wide = oracle.ref().ref_sgemm_kernel_choice(n, n) == 1
+        builds = [("stock", oracle.ref_sgemm)]
+        if not wide and rebase_ok:
+            builds.append(("rebased_test_only",
+                           lambda a, b, c, al, be: oracle.ref_sgemm_variant(5, a, b, c, al, be)))
+        row = {"kernel": "sgemm_128x256x8" if wide else "sgemm_128x128x8"}
+        for name, fn in builds:
+            C = torch.from_numpy(hC).cuda()
+            fn(A, B, C, ALPHA, BETA)
+            torch.cuda.synchronize()
+            got = C[torch.from_numpy(ids).long().cuda()].cpu().numpy()
+            exact = int(np.sum(got.view(np.uint32) == want.view(np.uint32)))
+            ms = _time_steps(torch, lambda: fn(A, B, C, ALPHA, BETA), _sweep_steps(n), warmup,
+                             flush)
+            t = statistics.mean(ms)
+            g = 2.0 * n ** 3 / (t * 1e-3) * 1e-9
+            row[name] = {"gflops": round(g, 1), "frac_of_simt_peak": round(g / peak_gflops, 4),
+                         "ms_per_step": round(t, 4), "steps": len(ms),
+                         "check": {"bit_exact": exact, "elements": int(want.size)}}
+            del C
+        out[str(n)] = row
+        del A, B, hC
+        torch.cuda.empty_cache()
+    return out
 
 
 def _reference_config_1024(torch, oracle, steps, warmup):
@@ -1078,6 +1196,8 @@ def main():
                          "(for labelled comparisons at sizes <= 2500)")
     ap.add_argument("--skip-config-1024", action="store_true",
                     help="reference arm only: skip the 1024^3 stock/rebased leg")
+    ap.add_argument("--skip-sweep", action="store_true",
+                    help="skip the square sweep leg (both arms)")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-split", action="store_true")
