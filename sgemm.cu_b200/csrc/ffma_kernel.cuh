@@ -227,10 +227,11 @@ __device__ __forceinline__ void load_stage_async4(const Operands& p, uint8_t* As
 }
 
 // Thread (wm, wn, lm, ln) owns rows m0 + WROWS wm + lm + 4i (i < TM) and the
-// float4 column groups n0 + wn*8*TN + 4ln + 32g (g < TN/4).
+// float4 column groups n0 + wn*8*TN + 4ln + 32g (g < TN/4).  One row at a
+// time, each C load right before its store.
 template <class C>
-__device__ __forceinline__ void epilogue(const Operands& p, int m0, int n0, int wm, int wn, int lm,
-                                         int ln, const float (&acc)[C::TM][C::TN]) {
+__device__ __forceinline__ void epilogue_rows(const Operands& p, int m0, int n0, int wm, int wn,
+                                              int lm, int ln, const float (&acc)[C::TM][C::TN]) {
     const int col0 = n0 + wn * 8 * C::TN + ln * 4;
 #pragma unroll
     for (int i = 0; i < C::TM; ++i) {
@@ -267,6 +268,93 @@ __device__ __forceinline__ void epilogue(const Operands& p, int m0, int n0, int 
     }
 }
 
+// The same outputs with the C loads batched: with beta != 0 every C value a
+// chunk of rows needs is loaded before the chunk's first store.  A store to C
+// may alias a later load of C as far as the compiler knows, so in
+// epilogue_rows each load waits for the store before it -- one DRAM round
+// trip per row, which on a lone CTA per SM is ~12% of a 1024^3 GEMM; a chunk
+// of BATCH values pays one.  The arithmetic per element is unchanged:
+// acc * alpha, then fma(C, beta, .).  Measured on a B200 against
+// epilogue_rows, same bits: beta = 0.5 +14% at 1000^3 and 1024^3, +2.6% at
+// 2048^3 and 3001^3, +0.6% at 4096^3 and 5003^3, level at 8192^3; beta = 0
+// unchanged.  epilogue() takes BATCH 0 for epilogue_rows: the grouped
+// kernel keeps it, since the batch's registers push that kernel (168 at
+// three CTAs per SM) into spills and made the 512-problem mix 2% slower.
+template <class C, int BATCH>
+__device__ __forceinline__ void epilogue_batched(const Operands& op, int m0, int n0, int wm,
+                                                 int wn, int lm, int ln,
+                                                 const float (&acc)[C::TM][C::TN]) {
+    // a private copy: the problem description may sit in global memory, where
+    // each store to C would otherwise force it to be read again
+    const Operands p = op;
+    const int col0 = n0 + wn * 8 * C::TN + ln * 4;
+    // rows per chunk: the chunk's BATCH old C values live in registers
+    constexpr int RC = BATCH / C::TN > 0 ? BATCH / C::TN : 1;
+#pragma unroll
+    for (int i0 = 0; i0 < C::TM; i0 += RC) {
+        float4 old[RC][C::TN / 4];
+        if (p.beta != 0.0f) {
+#pragma unroll
+            for (int ii = 0; ii < RC; ++ii) {
+                const int i = i0 + ii;
+                if (i >= C::TM) break;
+                const int row = m0 + wm * C::WROWS + lm + 4 * i;
+#pragma unroll
+                for (int g = 0; g < C::TN / 4; ++g) {
+                    const int col = col0 + 32 * g;
+                    old[ii][g] = make_float4(0.f, 0.f, 0.f, 0.f);
+                    if (row < p.m && p.vec_c && col + 3 < p.n)
+                        old[ii][g] = *reinterpret_cast<const float4*>(p.C + (int64_t)row * p.ldc +
+                                                                      col);
+                }
+            }
+        }
+#pragma unroll
+        for (int ii = 0; ii < RC; ++ii) {
+            const int i = i0 + ii;
+            if (i >= C::TM) break;
+            const int row = m0 + wm * C::WROWS + lm + 4 * i;
+            if (row >= p.m) continue;
+            float* crow = p.C + (int64_t)row * p.ldc;
+#pragma unroll
+            for (int g = 0; g < C::TN / 4; ++g) {
+                const int col = col0 + 32 * g;
+                float v[4];
+#pragma unroll
+                for (int e = 0; e < 4; ++e) v[e] = __fmul_rn(acc[i][4 * g + e], p.alpha);
+                if (p.vec_c && col + 3 < p.n) {
+                    if (p.beta != 0.0f) {
+                        const float4 o = old[ii][g];
+                        v[0] = fmaf(o.x, p.beta, v[0]);
+                        v[1] = fmaf(o.y, p.beta, v[1]);
+                        v[2] = fmaf(o.z, p.beta, v[2]);
+                        v[3] = fmaf(o.w, p.beta, v[3]);
+                    }
+                    *reinterpret_cast<float4*>(crow + col) = make_float4(v[0], v[1], v[2], v[3]);
+                } else {
+#pragma unroll
+                    for (int e = 0; e < 4; ++e) {
+                        if (col + e < p.n) {
+                            float out = v[e];
+                            if (p.beta != 0.0f) out = fmaf(crow[col + e], p.beta, out);
+                            crow[col + e] = out;
+                        }
+                    }
+                }
+            }
+        }
+    }
+}
+
+template <class C, int BATCH = 32>
+__device__ __forceinline__ void epilogue(const Operands& p, int m0, int n0, int wm, int wn,
+                                         int lm, int ln, const float (&acc)[C::TM][C::TN]) {
+    if constexpr (BATCH == 0)
+        epilogue_rows<C>(p, m0, n0, wm, wn, lm, ln, acc);
+    else
+        epilogue_batched<C, BATCH>(p, m0, n0, wm, wn, lm, ln, acc);
+}
+
 // Epilogue for C rows that are not 16-byte aligned (ldc % 4 != 0 or an
 // unaligned base), where float4 accesses are impossible and per-thread
 // scalar accesses would touch 4 rows x 4 sectors per warp instruction for
@@ -276,7 +364,7 @@ __device__ __forceinline__ void epilogue(const Operands& p, int m0, int n0, int 
 // segment per instruction.  The arithmetic per element is the epilogue's
 // (acc * alpha, then fma(C, beta, .)); only the thread that does it changes.
 // The caller must have made every warp finish reading the ring.
-template <class C>
+template <class C, int BATCH = 32>
 __device__ __forceinline__ void epilogue_staged(const Operands& p, int m0, int n0, int wm, int wn,
                                                 int lm, int ln, int warp, int lane,
                                                 const float (&acc)[C::TM][C::TN], uint8_t* smem) {
@@ -293,17 +381,55 @@ __device__ __forceinline__ void epilogue_staged(const Operands& p, int m0, int n
                 make_float4(acc[i][4 * g], acc[i][4 * g + 1], acc[i][4 * g + 2], acc[i][4 * g + 3]);
     __syncwarp();
     const int col0 = n0 + wn * W;
-    for (int r = 0; r < C::WROWS; ++r) {
-        const int row = m0 + wm * C::WROWS + r;
-        if (row >= p.m) break;
-        float* crow = p.C + (int64_t)row * p.ldc;
+    if constexpr (BATCH == 0) {  // one row at a time
+        for (int r = 0; r < C::WROWS; ++r) {
+            const int row = m0 + wm * C::WROWS + r;
+            if (row >= p.m) break;
+            float* crow = p.C + (int64_t)row * p.ldc;
 #pragma unroll
-        for (int t = 0; t < W / 32; ++t) {
-            const int col = col0 + lane + 32 * t;
-            if (col < p.n) {
-                float v = __fmul_rn(buf[r * LD + lane + 32 * t], p.alpha);
-                if (p.beta != 0.0f) v = fmaf(crow[col], p.beta, v);
-                crow[col] = v;
+            for (int t = 0; t < W / 32; ++t) {
+                const int col = col0 + lane + 32 * t;
+                if (col < p.n) {
+                    float v = __fmul_rn(buf[r * LD + lane + 32 * t], p.alpha);
+                    if (p.beta != 0.0f) v = fmaf(crow[col], p.beta, v);
+                    crow[col] = v;
+                }
+            }
+        }
+        return;
+    }
+    // rows in chunks of 8 whose C values are all loaded before the chunk's
+    // first store (see epilogue: one DRAM round trip per chunk, not per row)
+    constexpr int RC = 8;
+    for (int r0 = 0; r0 < C::WROWS; r0 += RC) {
+        float old[RC][W / 32];
+        if (p.beta != 0.0f) {
+#pragma unroll
+            for (int rr = 0; rr < RC; ++rr) {
+                const int row = m0 + wm * C::WROWS + r0 + rr;
+#pragma unroll
+                for (int t = 0; t < W / 32; ++t) {
+                    const int col = col0 + lane + 32 * t;
+                    old[rr][t] = (r0 + rr < C::WROWS && row < p.m && col < p.n)
+                                     ? p.C[(int64_t)row * p.ldc + col]
+                                     : 0.0f;
+                }
+            }
+        }
+#pragma unroll
+        for (int rr = 0; rr < RC; ++rr) {
+            const int r = r0 + rr;
+            const int row = m0 + wm * C::WROWS + r;
+            if (r >= C::WROWS || row >= p.m) break;
+            float* crow = p.C + (int64_t)row * p.ldc;
+#pragma unroll
+            for (int t = 0; t < W / 32; ++t) {
+                const int col = col0 + lane + 32 * t;
+                if (col < p.n) {
+                    float v = __fmul_rn(buf[r * LD + lane + 32 * t], p.alpha);
+                    if (p.beta != 0.0f) v = fmaf(old[rr][t], p.beta, v);
+                    crow[col] = v;
+                }
             }
         }
     }
@@ -321,16 +447,16 @@ __device__ __forceinline__ void compute_barrier() {
 // The epilogue for any C: float4 stores straight from registers when C rows
 // are 16-byte aligned, else the shared-memory staged form.  Called by every
 // compute thread of the CTA (the staged form has a barrier).
-template <class C>
+template <class C, int BATCH = 32>
 __device__ __forceinline__ void epilogue_any(const Operands& p, int m0, int n0, int wm, int wn,
                                              int lm, int ln, const float (&acc)[C::TM][C::TN],
                                              uint8_t* smem) {
     if (p.vec_c) {
-        epilogue<C>(p, m0, n0, wm, wn, lm, ln, acc);
+        epilogue<C, BATCH>(p, m0, n0, wm, wn, lm, ln, acc);
     } else {
         compute_barrier<C>();  // every warp is done reading the stage ring
         const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-        epilogue_staged<C>(p, m0, n0, wm, wn, lm, ln, warp, lane, acc, smem);
+        epilogue_staged<C, BATCH>(p, m0, n0, wm, wn, lm, ln, warp, lane, acc, smem);
     }
 }
 

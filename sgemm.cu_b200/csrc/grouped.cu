@@ -199,8 +199,10 @@ __device__ __forceinline__ bool run_item(const GParams& gp, const GProblem& pr, 
         cp_async_wait<0>();
     }
 
+    // epilogue with C read row by row (BATCH 0): batched C loads cost this
+    // kernel spills under its register cap
     if (pr.split == 1) {
-        ffma::epilogue_any<C>(pr.op, m0, n0, wm, wn, lm, ln, acc, smem);
+        ffma::epilogue_any<C, 0>(pr.op, m0, n0, wm, wn, lm, ln, acc, smem);
         return true;
     }
 
@@ -248,7 +250,7 @@ __device__ __forceinline__ bool run_item(const GParams& gp, const GProblem& pr, 
                 }
         }
         (void)NQ;
-        ffma::epilogue_any<C>(pr.op, m0, n0, wm, wn, lm, ln, acc, smem);
+        ffma::epilogue_any<C, 0>(pr.op, m0, n0, wm, wn, lm, ln, acc, smem);
     }
     return true;
 }
