@@ -38,3 +38,22 @@ def test_both_arms_build_config_with_the_same_function():
         calls = [n for n in ast.walk(fns[name]) if isinstance(n, ast.Call)
                  and isinstance(n.func, ast.Name) and n.func.id == "_config"]
         assert calls, f"{name} does not build its config with _config"
+
+
+def test_both_arms_sweep_the_reference_square_sizes():
+    """The sweep legs of both arms run the same sizes: 1024..16384 in steps of
+    1024 plus the sizes that are not multiples of a tile (1000, 3001, 5003)."""
+    src = open(os.path.join(ROOT, "bench.py")).read()
+    tree = ast.parse(src)
+    sizes = None
+    for node in tree.body:
+        if isinstance(node, ast.Assign) and any(getattr(t, "id", None) == "SWEEP_SIZES"
+                                                for t in node.targets):
+            sizes = eval(compile(ast.Expression(node.value), "bench.py", "eval"))
+    assert sizes == sorted([1000, 3001, 5003] + list(range(1024, 16385, 1024)))
+    fns = _functions()
+    for name, leg in (("run", "_sweep_leg"), ("run_reference", "_reference_sweep")):
+        calls = [n for n in ast.walk(fns[name]) if isinstance(n, ast.Call)
+                 and isinstance(n.func, ast.Name) and n.func.id == leg]
+        assert calls and any(isinstance(a, ast.Name) and a.id == "SWEEP_SIZES"
+                             for c in calls for a in c.args), name
