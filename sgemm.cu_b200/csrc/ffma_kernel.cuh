@@ -464,7 +464,72 @@ struct Params {
     Operands op;  // vec_c: C rows are 16-byte aligned (ldc % 4 == 0 and C aligned)
     int* status;
     int tiles_m, tiles_n;
+    // Accumulators carried between launches over consecutive k ranges (host
+    // pipeline): acc_in, when set, holds the unscaled sums of the k range
+    // before this one (row-major m x n, pitch ld_acc) and seeds every
+    // accumulator; acc_out, when set, receives this launch's unscaled sums
+    // instead of the alpha/beta epilogue (C is neither read nor written).
+    // Both 16-byte aligned with ld_acc % 4 == 0.
+    const float* acc_in;
+    float* acc_out;
+    int ld_acc;
 };
+
+// Thread (wm, wn, lm, ln) moves its accumulators between registers and an
+// m x n row-major buffer: acc[i][4g+e] is element (m0 + WROWS wm + lm + 4i,
+// n0 + 8 TN wn + 4 ln + 32 g + e).  A sum resumed from the buffer continues
+// the same k-ordered FMA chain, so a product computed over k ranges that
+// start on whole 32-deep k blocks has the bits of the product in one launch.
+template <class C, bool STORE>
+__device__ __forceinline__ void acc_move(const Operands& p, const float* in, float* out, int ld,
+                                         int m0, int n0, int wm, int wn, int lm, int ln,
+                                         float (&acc)[C::TM][C::TN]) {
+    const int col0 = n0 + wn * 8 * C::TN + ln * 4;
+#pragma unroll
+    for (int i = 0; i < C::TM; ++i) {
+        const int row = m0 + wm * C::WROWS + lm + 4 * i;
+        if (row >= p.m) continue;
+#pragma unroll
+        for (int g = 0; g < C::TN / 4; ++g) {
+            const int col = col0 + 32 * g;
+            const int64_t off = (int64_t)row * ld + col;
+            if (col + 3 < p.n) {
+                if constexpr (STORE) {
+                    *reinterpret_cast<float4*>(out + off) =
+                        make_float4(acc[i][4 * g], acc[i][4 * g + 1], acc[i][4 * g + 2],
+                                    acc[i][4 * g + 3]);
+                } else {
+                    const float4 v = *reinterpret_cast<const float4*>(in + off);
+                    acc[i][4 * g] = v.x;
+                    acc[i][4 * g + 1] = v.y;
+                    acc[i][4 * g + 2] = v.z;
+                    acc[i][4 * g + 3] = v.w;
+                }
+            } else {
+#pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                    if (col + e < p.n) {
+                        if constexpr (STORE)
+                            out[off + e] = acc[i][4 * g + e];
+                        else
+                            acc[i][4 * g + e] = in[off + e];
+                    }
+                }
+            }
+        }
+    }
+}
+
+// The end of a tile: the unscaled sums to acc_out, or the epilogue to C.
+template <class C>
+__device__ __forceinline__ void finish_tile(const Params& p, int m0, int n0, int wm, int wn,
+                                            int lm, int ln, float (&acc)[C::TM][C::TN],
+                                            uint8_t* smem) {
+    if (p.acc_out)
+        acc_move<C, true>(p.op, nullptr, p.acc_out, p.ld_acc, m0, n0, wm, wn, lm, ln, acc);
+    else
+        epilogue_any<C>(p.op, m0, n0, wm, wn, lm, ln, acc, smem);
+}
 
 template <class C>
 __global__ void __launch_bounds__(C::THREADS, C::MINB)
@@ -485,7 +550,14 @@ __global__ void __launch_bounds__(C::THREADS, C::MINB)
         if (tid == 0) {
             for (int s = 0; s < C::STAGES; ++s) {
                 mbar_init(&full_bar[s], 1);
-                mbar_init(&empty_bar[s], C::WM * C::WN);  // one arrival per compute warp
+                // one arrival per compute thread: each thread's arrive (release
+                // semantics) orders its own shared-memory reads of the stage
+                // before the producer's TMA may overwrite it.  One arrival per
+                // warp after __syncwarp() left other lanes' last loads of a
+                // stage unordered against the refill: on a B200 a warp's 32
+                // columns of a 28 x 256 tile occasionally took one k block's
+                // products from the next refill.
+                mbar_init(&empty_bar[s], C::COMPUTE_THREADS);
             }
             fence_barrier_init();
         }
@@ -503,6 +575,10 @@ __global__ void __launch_bounds__(C::THREADS, C::MINB)
                         atomicExch(p.status, SGEMM_B200_ERR_TIMEOUT);
                         break;
                     }
+                    // the compute threads' generic-proxy reads of the stage,
+                    // acquired through the empty barrier, before the async-proxy
+                    // (TMA) writes that refill it
+                    if (kb >= C::STAGES) fence_proxy_async_shared();
                     uint8_t* st = smem + s * C::STAGE_BYTES;
                     mbar_arrive_expect_tx(&full_bar[s], C::STAGE_TX);
                     tma_load_2d(st, &tmA, &full_bar[s], kb * C::BK, tm * C::BM);
@@ -527,6 +603,8 @@ __global__ void __launch_bounds__(C::THREADS, C::MINB)
         for (int i = 0; i < C::TM; ++i)
 #pragma unroll
             for (int j = 0; j < C::TN; ++j) acc[i][j] = 0.0f;
+        if (p.acc_in)
+            acc_move<C, false>(p.op, p.acc_in, nullptr, p.ld_acc, m0, n0, wm, wn, lm, ln, acc);
         for (int kb = 0; kb < nk; ++kb) {
             const int s = kb % C::STAGES;
             if (!mbar_wait(&full_bar[s], (kb / C::STAGES) & 1)) {
@@ -535,10 +613,9 @@ __global__ void __launch_bounds__(C::THREADS, C::MINB)
             }
             const uint8_t* st = smem + s * C::STAGE_BYTES;
             compute_stage<C>(st, st + C::A_BYTES, a_base, xa0, xa1, b_base, acc);
-            __syncwarp();
-            if (lane == 0) mbar_arrive(&empty_bar[s]);  // this warp is done with the stage
+            mbar_arrive(&empty_bar[s]);  // this thread is done with the stage
         }
-        epilogue_any<C>(p.op, m0, n0, wm, wn, lm, ln, acc, smem);
+        finish_tile<C>(p, m0, n0, wm, wn, lm, ln, acc, smem);
         return;
     }
 
@@ -561,6 +638,8 @@ __global__ void __launch_bounds__(C::THREADS, C::MINB)
     for (int i = 0; i < C::TM; ++i)
 #pragma unroll
         for (int j = 0; j < C::TN; ++j) acc[i][j] = 0.0f;
+    if (p.acc_in)
+        acc_move<C, false>(p.op, p.acc_in, nullptr, p.ld_acc, m0, n0, wm, wn, lm, ln, acc);
 
     if constexpr (C::LOADER == kLoaderTma) {
         int issued = 0;
@@ -594,7 +673,12 @@ __global__ void __launch_bounds__(C::THREADS, C::MINB)
             }
             // Every thread finished block kb-1, so its stage ((kb-1) % STAGES,
             // which is where block kb-1+STAGES == issued lands) may be refilled.
-            if (tid == 0 && kb > 0 && issued < nk) issue(issued++);
+            if (tid == 0 && kb > 0 && issued < nk) {
+                // every thread's generic-proxy reads of the stage (ordered by the
+                // barrier) before the async-proxy (TMA) writes that refill it
+                fence_proxy_async_shared();
+                issue(issued++);
+            }
             const uint8_t* st = smem + s * C::STAGE_BYTES;
             compute_stage<C>(st, st + C::A_BYTES, a_base, xa0, xa1, b_base, acc);
         }
@@ -631,7 +715,7 @@ __global__ void __launch_bounds__(C::THREADS, C::MINB)
         cp_async_wait<0>();
     }
 
-    epilogue_any<C>(p.op, m0, n0, wm, wn, lm, ln, acc, smem);
+    finish_tile<C>(p, m0, n0, wm, wn, lm, ln, acc, smem);
 }
 
 }  // namespace ffma

@@ -154,6 +154,9 @@ __device__ __forceinline__ bool run_item(const GParams& gp, const GProblem& pr, 
         };
         if (tid == 0) {
             const int depth = min(S, pr.depth);  // the bucket's stage count
+            // the previous item's generic reads of the ring (ordered by the CTA
+            // barrier between items) before these TMA refills
+            fence_proxy_async_shared();
             for (; issued < depth && issued < nkb; ++issued) issue(issued);
         }
         for (int j = 0; j < nkb; ++j) {
@@ -168,7 +171,10 @@ __device__ __forceinline__ bool run_item(const GParams& gp, const GProblem& pr, 
                 }
                 return false;
             }
-            if (tid == 0 && j > 0 && issued < nkb) issue(issued++);
+            if (tid == 0 && j > 0 && issued < nkb) {
+                fence_proxy_async_shared();  // generic reads of the stage before its TMA refill
+                issue(issued++);
+            }
             const uint8_t* st = smem + s * SLOT_BYTES;
             ffma::compute_stage<C>(st, st + C::A_BYTES, a_base, xa0, xa1, b_base, acc);
         }
