@@ -246,6 +246,20 @@ int sgemm_b200_host(int path, int m, int n, int k,
 int sgemm_b200_host_plan(int path, int m, int n, int k, int reads_c, int* rows,
                          int* chunk_cols, int max_chunks);
 
+/* Whether sgemm_b200_host takes its k-outer plan for this problem (host-only;
+ * plain path, large problems, when the plan's timing model puts it at least
+ * 3% ahead of the block plan above).  That plan streams A and B in k slices,
+ * running a whole-C GEMM per slice as soon as it lands with the FP32 sums
+ * carried between launches in device memory, then finishes the last k
+ * columns row band by row band with alpha/beta applied, each band returning
+ * while the next computes; slices start on whole 32-deep k blocks, so C has
+ * the same bits.  Writes k values of the sliced phase to *k_outer (0: the
+ * block plan runs), its slice count to *slices and the band height to *rows;
+ * returns a sgemm_b200_status.  sgemm_b200_host_planned always runs the block
+ * plan it is given.  No reference counterpart. */
+int sgemm_b200_host_plan_kouter(int path, int m, int n, int k, int reads_c, int* k_outer,
+                                int* slices, int* rows);
+
 /* sgemm_b200_host with the caller's block plan instead of the built-in one:
  * bands of `rows` rows (the last takes the rest; at most 16 bands) times
  * `nchunks` (1..4) column chunks of the widths in chunk_cols, which must sum

@@ -270,10 +270,22 @@ static void pack(const PackJob& a, const PackJob& b, cudaStream_t s) {
 
 int plain_launch(int cfg, int m, int n, int k, float alpha, const float* A, int lda,
                  const float* B, int ldb, float beta, float* C, int ldc, cudaStream_t stream) {
+    return plain_launch_acc(cfg, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, nullptr, nullptr,
+                            0, stream);
+}
+
+int plain_launch_acc(int cfg, int m, int n, int k, float alpha, const float* A, int lda,
+                     const float* B, int ldb, float beta, float* C, int ldc, const float* acc_in,
+                     float* acc_out, int ld_acc, cudaStream_t stream) {
     using namespace ffma;
     if (m == 0 || n == 0) return SGEMM_B200_OK;
     if (!device_is_sm100()) return SGEMM_B200_ERR_UNSUPPORTED;
-    const int mask = cfg < 0 ? pack_mask(m, n, k, A, lda, B, ldb) : 0;
+    if ((acc_in || acc_out) &&
+        (ld_acc < n || ld_acc % 4 != 0 || reinterpret_cast<uintptr_t>(acc_in) % 16 != 0 ||
+         reinterpret_cast<uintptr_t>(acc_out) % 16 != 0))
+        return SGEMM_B200_ERR_INVALID_ARG;
+    // carried accumulators: the caller keeps its operands TMA-aligned (no pack step)
+    const int mask = (cfg < 0 && !acc_in && !acc_out) ? pack_mask(m, n, k, A, lda, B, ldb) : 0;
     if (mask) {
         // Unaligned strides on a large problem: copy the offending operand(s) to
         // 16-byte-aligned rows (stream-ordered scratch from the library pool)
@@ -325,6 +337,9 @@ int plain_launch(int cfg, int m, int n, int k, float alpha, const float* A, int 
     if (!p.status) return SGEMM_B200_ERR_CUDA;
     p.tiles_m = div_up(m, cd.bm);
     p.tiles_n = div_up(n, cd.bn);
+    p.acc_in = acc_in;
+    p.acc_out = acc_out;
+    p.ld_acc = ld_acc;
 
     CUtensorMap tmA, tmB;
     std::memset(&tmA, 0, sizeof(tmA));

@@ -32,6 +32,7 @@
 #include <mutex>
 
 #include "common.h"
+#include "plain.h"
 
 namespace sgb {
 namespace host {
@@ -176,6 +177,96 @@ Plan make_plan(int path, int m, int n, int k, bool read_c) {
     return best;
 }
 
+// ------------------------------------------------------- k-outer plan --
+//
+// Plain path only.  Phase 1 streams A and B in k slices (A[:, slice] and
+// B[slice, :]) and runs a whole-C GEMM per slice as soon as its slice has
+// landed, carrying the unscaled FP32 sums between launches in an m x n device
+// buffer; phase 2 runs the last k2 = k - k1 columns band by band with the
+// alpha/beta epilogue, each band returning to the host while the next
+// computes.  The first GEMM starts after one thin slice instead of after a
+// whole band of A and chunk of B, and C's return overlaps phase 2.  Slices
+// start on multiples of 128 (whole 32-deep k blocks), so every element runs
+// the same k-ordered FMA chain as in one launch: the same bits.
+constexpr int kMaxSlices = 16;
+
+struct KPlan {
+    int k1;                   // phase 1 covers k in [0, k1); 0: not used
+    int nslices;              // phase-1 slices: [cut[s], cut[s + 1])
+    int cut[kMaxSlices + 1];
+    int rows;                 // phase-2 band height
+};
+
+static double kouter_model_ms(int m, int n, int k, bool read_c, const KPlan& p) {
+    constexpr double kPcieBytesPerS = 51e9, kFlopsPerS = 59e12;
+    double t_h = 0, t_c = 0, t_d = 0;
+    for (int s = 0; s < p.nslices; ++s) {
+        const double ks = p.cut[s + 1] - p.cut[s];
+        t_h += 4.0 * (double(m) + n) * ks / kPcieBytesPerS;
+        t_c = std::max(t_c, t_h) + 2.0 * double(m) * n * ks / kFlopsPerS;
+    }
+    const double k2 = k - p.k1;
+    t_h += 4.0 * k2 * n / kPcieBytesPerS;
+    for (int r0 = 0; r0 < m; r0 += p.rows) {
+        const double nr = std::min(p.rows, m - r0);
+        t_h += 4.0 * nr * k2 / kPcieBytesPerS + (read_c ? 4.0 * nr * n / kPcieBytesPerS : 0.0);
+        t_c = std::max(t_c, t_h) + 2.0 * nr * n * k2 / kFlopsPerS;
+        t_d = std::max(t_d, t_c) + 4.0 * nr * n / kPcieBytesPerS;
+    }
+    return t_d * 1e3;
+}
+
+// Candidates: a thin first slice (256 or 512 columns), then slices of about
+// 1024, and a phase 2 of 512..3072 columns in bands of the 2-D plan's height
+// or of 512..2048 rows.  Returns the plan with k1 == 0 when none applies.
+static KPlan make_kplan(int m, int n, int k, bool read_c, double* t_best) {
+    KPlan best{};
+    *t_best = 1e300;
+    if (k < 2048 || m < 1024 || n < 1024) return best;
+    for (int k2t : {512, 768, 1024, 1536, 2048, 3072}) {
+        const int k1 = (k - k2t) / 128 * 128;
+        if (k1 < 1024) continue;
+        for (int first : {256, 512}) {
+            KPlan p{};
+            p.k1 = k1;
+            p.cut[0] = 0;
+            p.cut[1] = first;
+            p.nslices = 1;
+            const int rest = k1 - first;
+            int parts = std::min(kMaxSlices - 1, (rest + 1023) / 1024);
+            const int w = (rest / parts + 127) / 128 * 128;
+            for (int c = first; c < k1 && p.nslices < kMaxSlices;) {
+                const int next = (p.nslices == kMaxSlices - 1) ? k1 : std::min(k1, c + w);
+                p.cut[++p.nslices] = next;
+                c = next;
+            }
+            if (p.cut[p.nslices] != k1) continue;
+            for (int rows : {band_rows(m, n), 512, 1024, 2048}) {
+                if (rows >= m || (m + rows - 1) / rows > kMaxBands) continue;
+                p.rows = rows;
+                const double t = kouter_model_ms(m, n, k, read_c, p);
+                if (t < *t_best) {
+                    *t_best = t;
+                    best = p;
+                }
+            }
+        }
+    }
+    return best;
+}
+
+// The k-outer plan replaces the 2-D plan when the model puts it at least 3%
+// ahead (plain path only: its kernels carry accumulators between launches).
+static bool choose_kplan(int path, int m, int n, int k, bool read_c, const Plan& plan,
+                         KPlan* out) {
+    if (path != SGEMM_B200_PATH_PLAIN) return false;
+    double t = 0;
+    const KPlan kp = make_kplan(m, n, k, read_c, &t);
+    if (kp.k1 <= 0 || !(t < 0.97 * model_ms(path, m, k, read_c, plan))) return false;
+    *out = kp;
+    return true;
+}
+
 // A plan is usable when its chunks cover n, its bands number at most
 // kMaxBands and its blocks at most kMaxBlocks (the engine's event arrays).
 static bool plan_ok(const Plan& p, int m, int n) {
@@ -189,6 +280,112 @@ static bool plan_ok(const Plan& p, int m, int n) {
     return cols == n;
 }
 
+// Streams: the H2D stream brings phase 1's slices in order, then B's last k2
+// rows, then per band A's last k2 columns and (beta != 0) C; phase 1 runs on
+// compute stream 0; phase 2's bands run on the four compute streams once
+// phase 1 and their operands are done; the D2H stream returns each band.
+static int run_kouter(int m, int n, int k, const float* alpha, const float* A, int lda,
+                      const float* B, int ldb, const float* beta, float* C, int ldc,
+                      cudaStream_t stream, const KPlan& kp) {
+    Engine* eng = engine();
+    if (!eng) return SGEMM_B200_ERR_CUDA;
+    cudaMemPool_t pool = library_pool();
+    if (!pool) return SGEMM_B200_ERR_CUDA;
+    const bool read_c = *beta != 0.0f;
+    const int bands = (m + kp.rows - 1) / kp.rows;
+    if (kp.nslices < 1 || kp.nslices > kMaxSlices || bands > kMaxBands ||
+        kp.nslices + bands > kMaxBlocks)
+        return SGEMM_B200_ERR_INVALID_ARG;
+    const int lda_d = (k + 3) / 4 * 4, ldb_d = (n + 3) / 4 * 4, ldc_d = (n + 3) / 4 * 4;
+    const size_t a_bytes = align_up(sizeof(float) * (size_t)m * lda_d, 256);
+    const size_t b_bytes = align_up(sizeof(float) * (size_t)k * ldb_d, 256);
+    const size_t c_bytes = align_up(sizeof(float) * (size_t)m * ldc_d, 256);
+
+    std::lock_guard<std::mutex> lock(eng->mu);
+    void* base = nullptr;
+    cudaError_t e = cudaMallocFromPoolAsync(&base, a_bytes + b_bytes + 2 * c_bytes, pool, stream);
+    if (e != cudaSuccess) return cuda_status(e);
+    char* p8 = static_cast<char*>(base);
+    float* dA = reinterpret_cast<float*>(p8);
+    float* dB = reinterpret_cast<float*>(p8 + a_bytes);
+    float* dC = reinterpret_cast<float*>(p8 + a_bytes + b_bytes);
+    float* dAcc = reinterpret_cast<float*>(p8 + a_bytes + b_bytes + c_bytes);
+
+    int status = SGEMM_B200_OK;
+    auto ok = [&](cudaError_t r) {
+        if (r != cudaSuccess && status == SGEMM_B200_OK) status = cuda_status(r);
+        return status == SGEMM_B200_OK;
+    };
+    auto gemm_ok = [&](int g) {
+        if (g != SGEMM_B200_OK && status == SGEMM_B200_OK) status = g;
+        return status == SGEMM_B200_OK;
+    };
+    const size_t f = sizeof(float);
+    cudaStream_t all[2 + kComputeStreams];
+    all[0] = eng->h2d;
+    all[1] = eng->d2h;
+    for (int i = 0; i < kComputeStreams; ++i) all[2 + i] = eng->comp[i];
+    if (ok(cudaEventRecord(eng->start, stream)))
+        for (cudaStream_t s : all) ok(cudaStreamWaitEvent(s, eng->start, 0));
+
+    // phase 1: whole-C GEMMs over the k slices, sums carried in dAcc
+    for (int s = 0; s < kp.nslices && status == SGEMM_B200_OK; ++s) {
+        const int c0 = kp.cut[s], ks = kp.cut[s + 1] - kp.cut[s];
+        if (!ok(cudaMemcpy2DAsync(dA + c0, f * lda_d, A + c0, f * lda, f * ks, m,
+                                  cudaMemcpyDefault, eng->h2d)) ||
+            !ok(cudaMemcpy2DAsync(dB + (size_t)c0 * ldb_d, f * ldb_d, B + (size_t)c0 * ldb,
+                                  f * ldb, f * n, ks, cudaMemcpyDefault, eng->h2d)) ||
+            !ok(cudaEventRecord(eng->in[s], eng->h2d)) ||
+            !ok(cudaStreamWaitEvent(eng->comp[0], eng->in[s], 0)))
+            break;
+        if (!gemm_ok(plain_launch_acc(-1, m, n, ks, *alpha, dA + c0, lda_d,
+                                      dB + (size_t)c0 * ldb_d, ldb_d, *beta, dC, ldc_d,
+                                      s > 0 ? dAcc : nullptr, dAcc, ldc_d, eng->comp[0])))
+            break;
+    }
+    ok(cudaEventRecord(eng->b_in[1], eng->comp[0]));  // phase 1 done
+    // phase 2: the last k2 columns band by band, alpha/beta applied, C returned
+    const int k1 = kp.k1, k2 = k - kp.k1;
+    if (status == SGEMM_B200_OK &&
+        ok(cudaMemcpy2DAsync(dB + (size_t)k1 * ldb_d, f * ldb_d, B + (size_t)k1 * ldb, f * ldb,
+                             f * n, k2, cudaMemcpyDefault, eng->h2d)))
+        ok(cudaEventRecord(eng->b_in[0], eng->h2d));
+    for (int b = 0; b < bands && status == SGEMM_B200_OK; ++b) {
+        const int r0 = b * kp.rows, nr = std::min(kp.rows, m - r0);
+        const int ev = kp.nslices + b;
+        cudaStream_t cs = eng->comp[b % kComputeStreams];
+        if (!ok(cudaMemcpy2DAsync(dA + (size_t)r0 * lda_d + k1, f * lda_d,
+                                  A + (size_t)r0 * lda + k1, f * lda, f * k2, nr,
+                                  cudaMemcpyDefault, eng->h2d)))
+            break;
+        if (read_c && !ok(cudaMemcpy2DAsync(dC + (size_t)r0 * ldc_d, f * ldc_d,
+                                            C + (size_t)r0 * ldc, f * ldc, f * n, nr,
+                                            cudaMemcpyDefault, eng->h2d)))
+            break;
+        if (!ok(cudaEventRecord(eng->in[ev], eng->h2d)) ||
+            !ok(cudaStreamWaitEvent(cs, eng->b_in[1], 0)) ||
+            !ok(cudaStreamWaitEvent(cs, eng->b_in[0], 0)) ||
+            !ok(cudaStreamWaitEvent(cs, eng->in[ev], 0)))
+            break;
+        if (!gemm_ok(plain_launch_acc(-1, nr, n, k2, *alpha, dA + (size_t)r0 * lda_d + k1, lda_d,
+                                      dB + (size_t)k1 * ldb_d, ldb_d, *beta,
+                                      dC + (size_t)r0 * ldc_d, ldc_d, dAcc + (size_t)r0 * ldc_d,
+                                      nullptr, ldc_d, cs)))
+            break;
+        if (!ok(cudaEventRecord(eng->done[b], cs)) ||
+            !ok(cudaStreamWaitEvent(eng->d2h, eng->done[b], 0)))
+            break;
+        ok(cudaMemcpy2DAsync(C + (size_t)r0 * ldc, f * ldc, dC + (size_t)r0 * ldc_d, f * ldc_d,
+                             f * n, nr, cudaMemcpyDefault, eng->d2h));
+    }
+    for (int i = 0; i < 2 + kComputeStreams; ++i) {
+        if (cudaEventRecord(eng->tail[i], all[i]) == cudaSuccess)
+            cudaStreamWaitEvent(stream, eng->tail[i], 0);
+    }
+    cudaFreeAsync(base, stream);
+    return status;
+}
+
 static int run(int path, int m, int n, int k, const float* alpha, const float* A, int lda,
                const float* B, int ldb, const float* beta, float* C, int ldc,
                cudaStream_t stream, const Plan* forced) {
@@ -199,6 +396,9 @@ static int run(int path, int m, int n, int k, const float* alpha, const float* A
 
     const bool read_c = *beta != 0.0f;  // beta == 0: C is written, never read
     const Plan plan = forced ? *forced : make_plan(path, m, n, k, read_c);
+    KPlan kp{};
+    if (!forced && choose_kplan(path, m, n, k, read_c, plan, &kp))
+        return run_kouter(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, stream, kp);
     const int bands = (m + plan.rows - 1) / plan.rows;
     // Device pitches: rows start on 16 bytes, so the TMA kernels take every block.
     const int lda_d = (k + 3) / 4 * 4, ldb_d = (n + 3) / 4 * 4, ldc_d = (n + 3) / 4 * 4;
@@ -324,6 +524,24 @@ extern "C" int sgemm_b200_host_planned(int path, int m, int n, int k, const floa
     }
     sgb::set_last_status(s);
     return s;
+}
+
+extern "C" int sgemm_b200_host_plan_kouter(int path, int m, int n, int k, int reads_c,
+                                           int* k_outer, int* slices, int* rows) {
+    if (m <= 0 || n <= 0 || k < 0 || !k_outer || !slices || !rows)
+        return SGEMM_B200_ERR_INVALID_ARG;
+    const sgb::host::Plan p = sgb::host::make_plan(path, m, n, k, reads_c != 0);
+    sgb::host::KPlan kp{};
+    if (sgb::host::choose_kplan(path, m, n, k, reads_c != 0, p, &kp)) {
+        *k_outer = kp.k1;
+        *slices = kp.nslices;
+        *rows = kp.rows;
+    } else {
+        *k_outer = 0;
+        *slices = 0;
+        *rows = 0;
+    }
+    return SGEMM_B200_OK;
 }
 
 extern "C" int sgemm_b200_host_plan(int path, int m, int n, int k, int reads_c, int* rows,

@@ -133,6 +133,8 @@ def _declare(lib: ctypes.CDLL) -> None:
     d("sgemm_b200_host_plan", _I, [_I, _I, _I, _I, _I, ctypes.POINTER(_I), ctypes.POINTER(_I),
                                    _I])
     d("sgemm_b200_host_planned", _I, [_I] + _GEMM_ARGS + [_I, ctypes.POINTER(_I), _I, _P])
+    d("sgemm_b200_host_plan_kouter", _I, [_I, _I, _I, _I, _I, ctypes.POINTER(_I),
+                                          ctypes.POINTER(_I), ctypes.POINTER(_I)])
     d("sgemm_b200_grouped_plan_create", _I,
       [ctypes.POINTER(_P), ctypes.POINTER(Problem), _I, ctypes.c_char_p])
     d("sgemm_b200_grouped_plan_launch", _I, [_P, _P, _I])
@@ -342,6 +344,17 @@ def host_plan(m: int, n: int, k: int, reads_c: bool = True, path="plain") -> tup
     if cnt < 0:
         raise SgemmError(-cnt, "sgemm_b200_host_plan")
     return r.value, [cols[i] for i in range(cnt)]
+
+
+def host_plan_kouter(m: int, n: int, k: int, reads_c: bool = True, path="plain") -> tuple:
+    """(k of the sliced phase, slices, band rows) of sgemm_host's k-outer plan
+    for this problem; (0, 0, 0) when it runs the block plan instead."""
+    p = PATHS[path] if isinstance(path, str) else int(path)
+    k1, sl, r = ctypes.c_int(0), ctypes.c_int(0), ctypes.c_int(0)
+    _check(lib().sgemm_b200_host_plan_kouter(p, m, n, k, int(reads_c), ctypes.byref(k1),
+                                             ctypes.byref(sl), ctypes.byref(r)),
+           "sgemm_b200_host_plan_kouter")
+    return k1.value, sl.value, r.value
 
 
 def fill_random(X, seed: int, tag: int, dist: int = DIST_UNIFORM_PM1, stream=None) -> None:

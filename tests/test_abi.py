@@ -140,6 +140,17 @@ def test_host_entry_validation_and_bands():
             assert -(-m // r) <= 16 and 1 <= len(chunks) <= 4 and sum(chunks) == n
             assert all(c % 128 == 0 and c >= 512 for c in chunks[:-1])
             assert len(chunks) == 1 or chunks[-1] >= 512
+    # the k-outer plan: plain path only, large problems with k >= 2048; its
+    # sliced phase ends on a multiple of 128 (whole 32-deep k blocks), leaves
+    # a k remainder for the banded phase, and its bands are whole 128-row tiles
+    k1, sl, r = sg.host_plan_kouter(8192, 8192, 8192)
+    assert 0 < k1 < 8192 and k1 % 128 == 0 and 1 <= sl <= 16 and r % 128 == 0
+    assert -(-8192 // r) <= 16
+    assert sg.host_plan_kouter(8192, 8192, 1024) == (0, 0, 0)  # short k: block plan
+    assert sg.host_plan_kouter(1000, 1000, 1000) == (0, 0, 0)
+    for path in ("bf16x6", "tf32x3"):
+        assert sg.host_plan_kouter(8192, 8192, 8192, True, path) == (0, 0, 0)
+    assert l.sgemm_b200_host_plan_kouter(0, 0, 4, 4, 1, None, None, None) == sg.ERR_INVALID_ARG
 
 def test_host_planned_rejects_invalid_plans():
     # plan checks run before any device work (pointers are never touched)

@@ -167,3 +167,21 @@ def test_host_rejects_bad_arguments():
     # nothing to do
     assert l.sgemm_b200_host(0, 0, 16, 32, alpha, A.data_ptr(), 32, B.data_ptr(), 16, beta,
                              C.data_ptr(), 16, None) == sg.OK
+
+
+@pytest.mark.parametrize("m,n,k,beta", [(4096, 4096, 4096, 0.5), (4096, 3000, 6000, 0.0),
+                                        (2500, 4224, 4100, 0.5)])
+def test_kouter_plan_equals_device(m, n, k, beta):
+    """Shapes where sgemm_host takes the k-outer plan (k slices streamed in,
+    sums carried between launches in device memory, then row bands with the
+    epilogue): the same bits as the device entry point, and NaN canaries
+    beyond C's columns untouched."""
+    k1, slices, rows = sg.host_plan_kouter(m, n, k, beta != 0)
+    assert 0 < k1 < k and k1 % 128 == 0 and slices >= 1 and rows % 128 == 0
+    A = oracle.fill(m, k, 61, 1, 0)
+    B = oracle.fill(k, n, 61, 2, 0)
+    C = oracle.fill(m, n, 61, 3, 0)
+    want = _device_result("plain", A, B, C, 1.5, beta)
+    bigC, got = _host_result("plain", A, B, C, 1.5, beta, lds=(k + 3, n + 5, n + 7))
+    assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+    assert np.isnan(bigC.numpy()[:, n:]).all()
