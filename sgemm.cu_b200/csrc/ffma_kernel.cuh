@@ -550,14 +550,7 @@ __global__ void __launch_bounds__(C::THREADS, C::MINB)
         if (tid == 0) {
             for (int s = 0; s < C::STAGES; ++s) {
                 mbar_init(&full_bar[s], 1);
-                // one arrival per compute thread: each thread's arrive (release
-                // semantics) orders its own shared-memory reads of the stage
-                // before the producer's TMA may overwrite it.  One arrival per
-                // warp after __syncwarp() left other lanes' last loads of a
-                // stage unordered against the refill: on a B200 a warp's 32
-                // columns of a 28 x 256 tile occasionally took one k block's
-                // products from the next refill.
-                mbar_init(&empty_bar[s], C::COMPUTE_THREADS);
+                mbar_init(&empty_bar[s], C::WM * C::WN);  // one arrival per compute warp
             }
             fence_barrier_init();
         }
@@ -575,9 +568,12 @@ __global__ void __launch_bounds__(C::THREADS, C::MINB)
                         atomicExch(p.status, SGEMM_B200_ERR_TIMEOUT);
                         break;
                     }
-                    // the compute threads' generic-proxy reads of the stage,
-                    // acquired through the empty barrier, before the async-proxy
-                    // (TMA) writes that refill it
+                    // The compute warps' generic-proxy reads of the stage,
+                    // acquired through the empty barrier, before the
+                    // async-proxy (TMA) writes that refill it.  Without this
+                    // fence a warp of the 28 x 256 tile occasionally took one
+                    // k block's products from the refill (one warp's 28 x 32
+                    // patch of C wrong, under concurrent launches on a B200).
                     if (kb >= C::STAGES) fence_proxy_async_shared();
                     uint8_t* st = smem + s * C::STAGE_BYTES;
                     mbar_arrive_expect_tx(&full_bar[s], C::STAGE_TX);
@@ -613,7 +609,8 @@ __global__ void __launch_bounds__(C::THREADS, C::MINB)
             }
             const uint8_t* st = smem + s * C::STAGE_BYTES;
             compute_stage<C>(st, st + C::A_BYTES, a_base, xa0, xa1, b_base, acc);
-            mbar_arrive(&empty_bar[s]);  // this thread is done with the stage
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&empty_bar[s]);  // this warp is done with the stage
         }
         finish_tile<C>(p, m0, n0, wm, wn, lm, ln, acc, smem);
         return;
