@@ -170,6 +170,8 @@ def test_host_rejects_bad_arguments():
 
 
 @pytest.mark.parametrize("m,n,k,beta", [(4096, 4096, 4096, 0.5), (4096, 3000, 6000, 0.0),
+                                        (3000, 4099, 4100, 0.5), (4097, 4101, 8192, 0.0),
+                                        (3001, 5003, 5000, 0.5),
                                         (2500, 4224, 4100, 0.5)])
 def test_kouter_plan_equals_device(m, n, k, beta):
     """Shapes where sgemm_host takes the k-outer plan (k slices streamed in,
