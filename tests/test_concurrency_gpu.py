@@ -120,3 +120,39 @@ def test_randomized_shapes_strides_and_scalars_bit_exact():
         if pads[2]:
             assert np.isnan(bigC[:, n:].cpu().numpy()).all(), f"trial {trial} wrote padding"
     assert sg.device_status() == sg.OK
+
+
+@pytest.mark.parametrize("name", ["tma_28x256_w4p_t7x8_s3", "tma_28x256_w4p_t7x8_s4",
+                                  "tma_128x64_w4p_t8x8_s4", "tma_128x64_w4_t8x8_s3"])
+def test_concurrent_band_gemms_bit_exact(name):
+    """Row bands of one problem as separate GEMMs, 16 in flight on four
+    streams, sixteen times over: each band's bits equal one whole launch's.
+    Compute warps read a shared-memory stage through the generic proxy and
+    the next TMA refill writes it through the async proxy; only a proxy fence
+    orders the two.  Without it, band GEMMs of the 28 x 256 producer tile
+    run concurrently like this occasionally returned one warp's 28 x 32
+    patch with one k block's products taken from the refill."""
+    torch = _torch()
+    m, n, k, rows = 8192, 4096, 3072, 512
+    cfg = sg.config_names().index(name)
+    A = torch.empty((m, k), device="cuda")
+    B = torch.empty((k, n), device="cuda")
+    C0 = torch.empty((m, n), device="cuda")
+    for t, X in ((1, A), (2, B), (3, C0)):
+        sg.fill_random(X, 71, t, sg.DIST_UNIFORM_PM1)
+    want = C0.clone()
+    sg.sgemm(A, B, want, 1.5, 0.5)
+    streams = [torch.cuda.Stream() for _ in range(4)]
+    torch.cuda.synchronize()
+    for _ in range(16):
+        C = C0.clone()
+        torch.cuda.synchronize()
+        for b in range(m // rows):
+            s = streams[b % 4]
+            with torch.cuda.stream(s):
+                sg.sgemm(A[b * rows:(b + 1) * rows], B, C[b * rows:(b + 1) * rows], 1.5, 0.5,
+                         stream=s, config=cfg)
+        torch.cuda.synchronize()
+        assert sg.device_status() == sg.OK
+        bad = (C.view(torch.int32) != want.view(torch.int32)).nonzero()
+        assert bad.numel() == 0, f"{name}: {bad.shape[0]} elements differ, first {bad[:3].tolist()}"
