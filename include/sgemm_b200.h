@@ -222,10 +222,13 @@ int sgemm_b200_gemm(int path, int m, int n, int k,
  * (test.cu:70-80, benchmark.cu:69-73): the library stages the operands in
  * device memory itself, cutting C into blocks (row bands x column chunks,
  * see sgemm_b200_host_plan) so that the host-to-device copies, the block
- * GEMMs (four streams) and the device-to-host copies overlap.  `path` is a
- * sgemm_b200_path; each block is the same GEMM sgemm_b200_gemm() runs, so C
- * is bit-identical to copying everything and calling it once.  Device memory:
- * A, B and C, from the library's stream-ordered pool.  Stream-ordered on
+ * GEMMs (four streams) and the device-to-host copies overlap; large plain
+ * problems take the k-outer plan instead (see sgemm_b200_host_plan_kouter).
+ * `path` is a sgemm_b200_path; each block is the same GEMM sgemm_b200_gemm()
+ * runs, and k slices start on whole 32-deep k blocks, so C is bit-identical
+ * to copying everything and calling it once.  Device memory: A, B and C from
+ * the library's stream-ordered pool (and, for the k-outer plan, an m x n
+ * buffer of FP32 sums).  Stream-ordered on
  * `stream`: C on the host is final once `stream` has synchronised.
  * Page-locked host memory is needed for the overlap (pageable memory works
  * but copies synchronously).  beta == 0 never reads C.  Not for use inside
