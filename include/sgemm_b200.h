@@ -242,7 +242,8 @@ int sgemm_b200_host(int path, int m, int n, int k,
                     float* C, int ldc,
                     sgemm_b200_stream_t stream);
 
-/* Block plan sgemm_b200_host uses for this problem (host-only): writes the
+/* Block plan sgemm_b200_host uses for this problem when it does not take the
+ * k-outer plan (sgemm_b200_host_plan_kouter; host-only): writes the
  * rows per band to *rows and the widths of up to max_chunks column chunks to
  * chunk_cols, and returns the number of chunks (m rows and one chunk of n
  * columns when it does not split), or a negated sgemm_b200_status. */
